@@ -1,0 +1,239 @@
+"""B200 DCX suffix-array builder: Python mirror of the reference's construction path.
+
+The reference (lightweight_dcx) builds a suffix array through
+``PDCX<char, index, DC>::compute_sa(std::vector<char>&) -> std::vector<index>``
+(lightweight_dcx/src/pdcx/pdcx.hpp:529), configured by ``PDCXConfig``
+(pdcx/config.hpp:27-60) and selected by the cli's ``--dcx`` flag
+(executables/cli.cpp:598-653).  This module exposes the same operation over the
+C ABI of ``lib/libdcxgpu.so`` (include/dcx_gpu.h):
+
+    from distributed_suffix_sorting_evaluation_b200 import PDCX, PDCXConfig
+    sa = PDCX(PDCXConfig(dc=39)).compute_sa(text_bytes)          # numpy uint64
+
+Errors are raised as ``DcxError`` carrying the C status code (the reference
+exits the process instead; the library never does).  There is no CPU fallback:
+without the compiled library or a GPU every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libdcxgpu.so")
+
+DCX_OK = 0
+DCX_ERR_ARG = -1
+DCX_ERR_ALPHABET = -2
+DCX_ERR_OOM = -3
+DCX_ERR_BUDGET = -4
+DCX_ERR_TIMEOUT = -5
+DCX_ERR_CUDA = -6
+DCX_ERR_INTERNAL = -7
+DCX_ERR_BUSY = -8
+DCX_ERR_NOTFOUND = -9
+
+DCX_HOST_PTRS = 0
+DCX_DEVICE_PTRS = 1
+DCX_NO_PACKING = 2
+DCX_NO_REMAP = 4
+
+SUPPORTED_DC = (3, 7, 13, 21, 31, 39, 57, 73, 91, 95, 133)
+
+# Every exported symbol of include/dcx_gpu.h (checked by the CPU test suite).
+EXPORTED = (
+    "dcx_ctx_create", "dcx_ctx_destroy", "dcx_set_option", "dcx_build_sa", "dcx_build_sa_strict",
+    "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
+    "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
+)
+
+
+class DcxError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__(f"dcx error {code}: {what}")
+
+
+class DcxStats(ctypes.Structure):
+    _fields_ = [
+        ("ms_total", ctypes.c_double), ("ms_phase0", ctypes.c_double), ("ms_phase12", ctypes.c_double),
+        ("ms_phase3", ctypes.c_double), ("ms_phase4", ctypes.c_double), ("ms_h2d", ctypes.c_double),
+        ("ms_d2h", ctypes.c_double), ("bytes_alg", ctypes.c_uint64), ("bytes_radix", ctypes.c_uint64),
+        ("ms_radix", ctypes.c_double), ("radix_passes", ctypes.c_uint64), ("radix_keys", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64), ("levels", ctypes.c_uint32),
+        ("sigma", ctypes.c_uint32), ("level0_samples", ctypes.c_uint64), ("level0_last_rank", ctypes.c_uint64),
+        ("level0_recursion", ctypes.c_int), ("level0_reduction", ctypes.c_double),
+        ("tie_groups", ctypes.c_uint64), ("tie_elements", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Loads lib/libdcxgpu.so (building it first when absent and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        from . import build as _b
+        _b.build()
+    lib = ctypes.CDLL(p)
+    vp, u64, u32, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int
+    lib.dcx_ctx_create.argtypes = [ctypes.POINTER(vp), i32, u64]
+    lib.dcx_ctx_destroy.argtypes = [vp]
+    lib.dcx_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_double]
+    lib.dcx_build_sa.argtypes = [vp, vp, u64, i32, i32, vp, u32]
+    lib.dcx_build_sa_strict.argtypes = [vp, vp, u64, i32, i32, vp, u32]
+    lib.dcx_get_stats.argtypes = [vp, ctypes.POINTER(DcxStats)]
+    lib.dcx_get_trace.argtypes = [vp, ctypes.POINTER(u64), vp, vp, u64]
+    lib.dcx_build_sa_batch.argtypes = [vp, vp, vp, u32, i32, i32, vp, u32]
+    lib.dcx_serve_submit.argtypes = [vp, vp, u64, i32, i32, ctypes.POINTER(u64)]
+    lib.dcx_serve_poll.argtypes = [vp, u64, vp, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]
+    lib.dcx_serve_release.argtypes = [vp, u64]
+    lib.dcx_serve_drain.argtypes = [vp]
+    lib.dcx_strerror.argtypes = [i32]
+    lib.dcx_strerror.restype = ctypes.c_char_p
+    lib.dcx_dc_table.argtypes = [i32, vp, vp, vp, vp]
+    lib.dcx_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != DCX_OK:
+        raise DcxError(rc, load_library().dcx_strerror(rc).decode())
+
+
+def dc_table(X: int):
+    """(DC, NEXT_RANK, cmpDepthRanks[X][X][3]) from the library (host-only call)."""
+    lib = load_library()
+    D = ctypes.c_uint32()
+    dc = np.zeros(32, np.uint32)
+    nr = np.zeros(X, np.uint32)
+    cmp = np.zeros(X * X * 3, np.uint32)
+    _check(lib.dcx_dc_table(X, ctypes.byref(D), dc.ctypes.data, nr.ctypes.data, cmp.ctypes.data))
+    return dc[: D.value].copy(), nr, cmp.reshape(X, X, 3)
+
+
+def sa_dtype_bytes(width: int) -> int:
+    return {32: 4, 40: 5, 64: 8}[width]
+
+
+def unpack_sa(raw: np.ndarray, width: int, n: int) -> np.ndarray:
+    """Raw SA bytes of the given width -> uint64 array."""
+    if width == 32:
+        return raw.view(np.uint32)[:n].astype(np.uint64)
+    if width == 64:
+        return raw.view(np.uint64)[:n].copy()
+    b = raw.view(np.uint8)[: 5 * n].reshape(n, 5).astype(np.uint64)
+    return b[:, 0] | (b[:, 1] << 8) | (b[:, 2] << 16) | (b[:, 3] << 24) | (b[:, 4] << 32)
+
+
+class Context:
+    """One device context (streams, memory pool, look-back scratch, statistics)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self.lib.dcx_ctx_create(ctypes.byref(h), device, hbm_budget_bytes))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dcx_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_option(self, name: str, value: float):
+        _check(self.lib.dcx_set_option(self.h, name.encode(), float(value)))
+
+    def build_sa_raw(self, text, dc: int = 39, sa_width: int = 40, packing: bool = True, strict: bool = False,
+                     remap: bool = True) -> np.ndarray:
+        """SA of host bytes; returns the raw little-endian bytes of sa_width bits per entry."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        n = t.size
+        out = np.zeros(max(n, 1) * sa_dtype_bytes(sa_width), np.uint8)
+        flags = DCX_HOST_PTRS | (0 if packing else DCX_NO_PACKING) | (0 if remap else DCX_NO_REMAP)
+        fn = self.lib.dcx_build_sa_strict if strict else self.lib.dcx_build_sa
+        _check(fn(self.h, t.ctypes.data if n else None, n, dc, sa_width, out.ctypes.data, flags))
+        return out[: n * sa_dtype_bytes(sa_width)]
+
+    def build_sa(self, text, dc: int = 39, sa_width: int = 64, **kw) -> np.ndarray:
+        raw = self.build_sa_raw(text, dc=dc, sa_width=sa_width, **kw)
+        n = raw.size // sa_dtype_bytes(sa_width)
+        return unpack_sa(raw, sa_width, n)
+
+    def build_sa_device(self, text_ptr: int, n: int, sa_ptr: int, dc: int = 39, sa_width: int = 32,
+                        packing: bool = True):
+        """SA of a device-resident text into a device buffer (both raw CUDA pointers)."""
+        flags = DCX_DEVICE_PTRS | (0 if packing else DCX_NO_PACKING)
+        _check(self.lib.dcx_build_sa(self.h, ctypes.c_void_p(text_ptr), n, dc, sa_width, ctypes.c_void_p(sa_ptr),
+                                     flags))
+
+    def stats(self) -> dict:
+        s = DcxStats()
+        _check(self.lib.dcx_get_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def trace(self):
+        """Level-0 names and unique flags of the last build with option trace=1."""
+        m = ctypes.c_uint64()
+        _check(self.lib.dcx_get_trace(self.h, ctypes.byref(m), None, None, 0))
+        names = np.zeros(max(m.value, 1), np.uint32)
+        uniq = np.zeros(max(m.value, 1), np.uint8)
+        _check(self.lib.dcx_get_trace(self.h, ctypes.byref(m), names.ctypes.data, uniq.ctypes.data, names.size))
+        return names[: m.value], uniq[: m.value]
+
+
+@dataclass
+class PDCXConfig:
+    """The fields of the reference's PDCXConfig that change the GPU build's behaviour.
+    Distribution/sorter knobs of the reference (atomic_sorter, buckets, splitters,
+    chunks) have no meaning on one GPU; they are accepted by the cli and ignored."""
+    dc: int = 39
+    use_char_packing_samples: bool = True
+    use_char_packing_merging: bool = True
+    discarding_threshold: float = 0.7
+    sa_width: int = 40
+    device: int = 0
+    recursion_dc: int = 3
+    extra: dict = field(default_factory=dict)
+
+
+class PDCX:
+    """Mirror of PDCX<char_type, index_type, DC> for the construction call."""
+
+    def __init__(self, config: PDCXConfig | None = None, context: Context | None = None):
+        self.config = config or PDCXConfig()
+        if self.config.dc not in SUPPORTED_DC:
+            raise DcxError(DCX_ERR_ARG, f"unsupported DC X={self.config.dc}")
+        self.ctx = context or Context(self.config.device)
+        self.ctx.set_option("discarding_threshold", self.config.discarding_threshold)
+        self.ctx.set_option("recursion_dc", self.config.recursion_dc)
+
+    def compute_sa(self, local_string) -> np.ndarray:
+        packing = self.config.use_char_packing_samples or self.config.use_char_packing_merging
+        return self.ctx.build_sa(local_string, dc=self.config.dc, sa_width=64, packing=packing)
+
+    def stats(self) -> dict:
+        return self.ctx.stats()

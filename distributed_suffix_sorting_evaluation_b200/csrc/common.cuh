@@ -1,0 +1,165 @@
+// Shared device/host helpers of the DCX engine: error plumbing, launch
+// bookkeeping, warp/block scans and the device-wide three-phase scan used by
+// naming, compaction and group detection.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "dcx_gpu.h"
+
+namespace dcx {
+
+// Host-side error carrying a dcx status code; every C-ABI entry converts it.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define DCX_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            if (e_ == cudaErrorMemoryAllocation)                                         \
+                throw ::dcx::Error(DCX_ERR_OOM, std::string("out of device memory: ") + #call); \
+            throw ::dcx::Error(DCX_ERR_CUDA, std::string(cudaGetErrorString(e_)) + " at " +    \
+                                                 __FILE__ + ":" + std::to_string(__LINE__)); \
+        }                                                                                \
+    } while (0)
+
+#define DCX_CHECK_LAUNCH() DCX_CUDA(cudaGetLastError())
+
+inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+// Device error word bits (set by kernels that give up a bounded wait or detect
+// an out-of-range index; the host turns a nonzero word into an error code).
+enum : uint32_t { DEV_ERR_TIMEOUT = 1u, DEV_ERR_RANGE = 2u };
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Inclusive warp scan of a 32-bit sum.
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane_id() >= (uint32_t)o) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ uint64_t warp_incl_scan64(uint64_t v) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane_id() >= (uint32_t)o) v += t;
+    }
+    return v;
+}
+
+// Exclusive block scan of one value per thread; returns the exclusive prefix and
+// writes the block total.  `smem` needs THREADS/32 + 1 slots.
+template <int THREADS, typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T* smem, T& total) {
+    constexpr int WARPS = THREADS / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) smem[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < WARPS ? smem[lane] : T(0);
+        T wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < WARPS) smem[lane] = wi - w;
+        if (lane == WARPS - 1) smem[WARPS] = wi;
+    }
+    __syncthreads();
+    T r = smem[warp] + inc - v;
+    total = smem[WARPS];
+    __syncthreads();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan in three phases (tile reduce, scan of tile sums,
+// tile rescan).  Op supplies   T load(uint64_t i)   and
+//   void store(uint64_t i, T exclusive_prefix, T value)   for i < n.
+// No inter-CTA waits, so nothing can spin.
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 16;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <typename T, typename Op>
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(Op op, uint64_t n, T* tile_sums) {
+    __shared__ T sm[SCAN_THREADS / 32 + 1];
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+    T acc = T(0);
+#pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        uint64_t i = base + (uint64_t)it * SCAN_THREADS + threadIdx.x;
+        if (i < n) acc += op.load(i);
+    }
+    T total;
+    block_excl_scan<SCAN_THREADS>(acc, sm, total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Single-CTA exclusive scan of the tile sums (in place); also writes the grand total.
+template <typename T>
+__global__ __launch_bounds__(1024) void k_scan_tile_sums(T* sums, uint64_t count, T* grand_total) {
+    __shared__ T sm[1024 / 32 + 1];
+    T carry = T(0);
+    for (uint64_t base = 0; base < count; base += 1024) {
+        uint64_t i = base + threadIdx.x;
+        T v = i < count ? sums[i] : T(0);
+        T total;
+        T ex = block_excl_scan<1024>(v, sm, total);
+        if (i < count) sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0 && grand_total) *grand_total = carry;
+}
+
+template <typename T, typename Op>
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(Op op, uint64_t n, const T* tile_prefix) {
+    __shared__ T sm[SCAN_THREADS / 32 + 1];
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+    T vals[SCAN_ITEMS];
+    T acc = T(0);
+    // blocked layout: thread t owns items [t*ITEMS, (t+1)*ITEMS) of the tile
+#pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        uint64_t i = base + it;
+        vals[it] = i < n ? op.load(i) : T(0);
+        acc += vals[it];
+    }
+    T total;
+    T ex = block_excl_scan<SCAN_THREADS>(acc, sm, total);
+    T run = tile_prefix[blockIdx.x] + ex;
+#pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        uint64_t i = base + it;
+        if (i < n) op.store(i, run, vals[it]);
+        run += vals[it];
+    }
+}
+
+}  // namespace dcx

@@ -1,0 +1,1210 @@
+// B200 DCX suffix-array engine: host orchestration of one DCX level and the C ABI.
+//
+// One level follows PDCX::compute_sa (lightweight_dcx/src/pdcx/pdcx.hpp:529-941):
+//   phase 0  lengths, dummy sample, key plan           (pdcx.hpp:473-510)
+//   phase 1  sort suffixes by their first L chars       (sample_string.hpp:129-239)
+//   phase 2  lexicographic names + unique flags         (compute_ranks.hpp:89-134)
+//   phase 3  recursion unless names are distinct        (pdcx.hpp:146-462,743-757)
+//   phase 4  order ties by difference-cover ranks       (merge_samples.hpp:87-109,262-306)
+// Design difference from the reference: phase 1 and phase 4 share ONE sort.  All
+// n+1 suffixes (position n is the empty suffix / dummy sample) are radix sorted
+// by their L-char window, which orders the samples exactly as phase 1 needs them
+// (a sample sort restricted to samples) and orders every non-tied suffix finally
+// (the reference's phase-4 comparator compares the same packed chars first).
+// Only suffixes whose whole window ties need the rank comparison afterwards.
+// The window sort runs as a short prefix radix sort followed by refinement sorts
+// of just the tied elements (group number, next chars).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "keys.cuh"
+#include "level_kernels.cuh"
+#include "radix.cuh"
+#include "segsort.cuh"
+#include "small_sa.cuh"
+
+namespace dcx {
+
+// ---------------------------------------------------------------------------
+// Difference covers of lightweight_dcx/src/pdcx/difference_cover.hpp:14-5126 (the
+// sets only; IN_DC, NEXT_RANK and cmpDepthRanks are generated in closed form).
+// ---------------------------------------------------------------------------
+struct DcHost {
+    uint32_t X = 0, D = 0;
+    std::vector<uint32_t> dc, next_rank, cmp;  // cmp: [X][X][3]
+    std::vector<uint8_t> in_dc;
+};
+
+static bool cover_of(uint32_t X, std::vector<uint32_t>& s) {
+    switch (X) {
+        case 3: s = {1, 2}; return true;
+        case 7: s = {1, 2, 4}; return true;
+        case 13: s = {1, 2, 4, 10}; return true;
+        case 21: s = {1, 2, 7, 9, 19}; return true;
+        case 31: s = {1, 2, 4, 9, 13, 19}; return true;
+        case 39: s = {1, 2, 17, 21, 23, 28, 31}; return true;
+        case 57: s = {1, 2, 10, 12, 15, 36, 40, 52}; return true;
+        case 73: s = {1, 2, 4, 8, 16, 32, 37, 55, 64}; return true;
+        case 91: s = {1, 2, 8, 17, 28, 57, 61, 69, 71, 74}; return true;
+        case 95: s = {1, 2, 6, 9, 19, 21, 30, 32, 46, 62, 68}; return true;
+        case 133: s = {1, 2, 33, 43, 45, 49, 52, 60, 73, 78, 98, 112}; return true;
+        default: return false;
+    }
+}
+
+static bool make_dc(uint32_t X, DcHost& t) {
+    if (!cover_of(X, t.dc)) return false;
+    t.X = X;
+    t.D = (uint32_t)t.dc.size();
+    t.in_dc.assign(X, 0);
+    for (uint32_t c : t.dc) t.in_dc[c] = 1;
+    t.next_rank.assign(X, 0);
+    for (uint32_t r = 0; r < X; r++)
+        for (uint32_t c : t.dc) t.next_rank[r] += c < r;
+    t.cmp.assign((size_t)X * X * 3, 0);
+    for (uint32_t i = 0; i < X; i++)
+        for (uint32_t j = 0; j < X; j++) {
+            uint32_t l = 0;
+            while (!(t.in_dc[(i + l) % X] && t.in_dc[(j + l) % X])) l++;
+            uint32_t r1 = 0, r2 = 0;
+            for (uint32_t k = 0; k < l; k++) {
+                r1 += t.in_dc[(i + k) % X];
+                r2 += t.in_dc[(j + k) % X];
+            }
+            uint32_t* e = &t.cmp[((size_t)i * X + j) * 3];
+            e[0] = l;
+            e[1] = r1;
+            e[2] = r2;
+        }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Key plans: number of chars of base B that fit in w words, and the chunking.
+// ---------------------------------------------------------------------------
+struct BigUInt {  // little-endian 32-bit limbs
+    std::vector<uint32_t> l{1};
+    void mul(uint32_t f) {
+        uint64_t carry = 0;
+        for (auto& x : l) {
+            uint64_t t = (uint64_t)x * f + carry;
+            x = (uint32_t)t;
+            carry = t >> 32;
+        }
+        if (carry) l.push_back((uint32_t)carry);
+    }
+    uint32_t bits_of_minus_one() const {  // bit length of (this - 1), this >= 1
+        std::vector<uint32_t> v = l;
+        for (auto& x : v) {
+            if (x) {
+                x--;
+                break;
+            }
+            x = 0xffffffffu;
+        }
+        while (v.size() > 1 && v.back() == 0) v.pop_back();
+        uint32_t top = v.back();
+        uint32_t b = 0;
+        while (top) {
+            b++;
+            top >>= 1;
+        }
+        return (uint32_t)(v.size() - 1) * 32 + b;
+    }
+};
+
+static uint32_t key_bits(uint64_t B, uint32_t P) {
+    BigUInt x;
+    for (uint32_t i = 0; i < P; i++) x.mul((uint32_t)B);
+    return std::max<uint32_t>(1, x.bits_of_minus_one());
+}
+
+static uint32_t max_chars_in(uint64_t B, uint32_t words) {
+    uint32_t P = 0;
+    BigUInt x;
+    while (true) {
+        BigUInt y = x;
+        y.mul((uint32_t)B);
+        if (y.bits_of_minus_one() > 32 * words) break;
+        x = y;
+        P++;
+        if (P > 4096) break;
+    }
+    return P;
+}
+
+static KeyPlan make_plan(uint64_t B, uint32_t P) {
+    KeyPlan p{};
+    p.base = (uint32_t)B;
+    p.chars = P;
+    p.kw = (key_bits(B, P) + 31) / 32;
+    uint32_t kmax = 1;
+    {
+        uint64_t v = B;
+        while (v * B <= 0xffffffffull) {
+            v *= B;
+            kmax++;
+        }
+    }
+    uint32_t left = P;
+    p.nchunks = 0;
+    while (left) {
+        uint32_t len = std::min(left, kmax);
+        uint64_t mul = 1;
+        for (uint32_t i = 0; i < len; i++) mul *= B;
+        if (p.nchunks >= (uint32_t)MAX_CHUNKS) throw Error(DCX_ERR_INTERNAL, "key plan too long");
+        p.chunk_len[p.nchunks] = len;
+        p.chunk_mul[p.nchunks] = (uint32_t)mul;
+        p.nchunks++;
+        left -= len;
+    }
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Context: stream, memory accounting, scratch, options, statistics.
+// ---------------------------------------------------------------------------
+struct Options {
+    double discarding_threshold = 0.7;
+    uint32_t recursion_dc = 3;
+    uint32_t small_threshold = SMALL_MAX;
+    uint32_t prefix_chars = 0;
+    int trace = 0;
+    uint32_t spin_limit = 1u << 24;
+};
+
+struct Ctx;
+
+template <typename T>
+struct DBuf {
+    Ctx* c = nullptr;
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(Ctx* ctx, size_t count);
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept { *this = std::move(o); }
+    DBuf& operator=(DBuf&& o) noexcept;
+    ~DBuf() { reset(); }
+    void reset();
+    T* get() const { return p; }
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t in_use = 0, peak = 0;
+    Options opt;
+    dcx_stats st{};
+    // scratch
+    uint32_t* d_hist = nullptr;     // [16 * RADIX]
+    uint32_t* d_base = nullptr;     // [16 * RADIX]
+    uint32_t* d_tiles = nullptr;    // [16]
+    uint32_t* d_err = nullptr;      // [1]
+    unsigned long long* d_h256 = nullptr;
+    uint64_t* d_lookback = nullptr;
+    size_t lookback_tiles = 0;
+    uint32_t epoch = 0;
+    uint32_t* h_pinned = nullptr;   // pinned staging for small D2H
+    std::map<uint32_t, DcHost> dc_host;
+    std::map<uint32_t, DcFlags*> dc_flags_dev;  // per X (samples_before filled per level on a copy)
+    std::map<uint32_t, DcDev*> dc_dev;
+    // trace of level 0
+    std::vector<uint32_t> trace_names;
+    std::vector<uint8_t> trace_uniq;
+    std::mutex build_mu;
+
+    void* alloc(size_t bytes) {
+        if (bytes == 0) bytes = 16;
+        bytes = (bytes + 255) & ~size_t(255);
+        if (budget && in_use + bytes > budget)
+            throw Error(DCX_ERR_BUDGET, "device footprint above the context budget");
+        void* p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(DCX_ERR_OOM, "cudaMallocAsync failed for " + std::to_string(bytes) + " bytes");
+        }
+        in_use += bytes;
+        peak = std::max(peak, in_use);
+        return p;
+    }
+    void release(void* p, size_t bytes) {
+        if (!p) return;
+        if (bytes == 0) bytes = 16;
+        bytes = (bytes + 255) & ~size_t(255);
+        cudaFreeAsync(p, stream);
+        in_use -= bytes;
+    }
+    void launched(uint64_t k = 1) { st.kernel_launches += k; }
+    void alg(uint64_t b) { st.bytes_alg += b; }
+};
+
+template <typename T>
+DBuf<T>::DBuf(Ctx* ctx, size_t count) : c(ctx), n(count) {
+    p = static_cast<T*>(ctx->alloc(count * sizeof(T)));
+}
+template <typename T>
+DBuf<T>& DBuf<T>::operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+        reset();
+        c = o.c;
+        p = o.p;
+        n = o.n;
+        o.p = nullptr;
+        o.n = 0;
+    }
+    return *this;
+}
+template <typename T>
+void DBuf<T>::reset() {
+    if (p && c) c->release(p, n * sizeof(T));
+    p = nullptr;
+    n = 0;
+}
+
+static int grid_for(uint64_t n, int threads, int max_blocks = 148 * 16) {
+    uint64_t b = div_up(std::max<uint64_t>(n, 1), threads);
+    return (int)std::min<uint64_t>(b, (uint64_t)max_blocks);
+}
+
+template <typename T>
+static T d2h_scalar(Ctx& c, const T* dptr) {
+    T v;
+    DCX_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    return v;
+}
+
+static void check_device_error(Ctx& c) {
+    uint32_t e = d2h_scalar(c, c.d_err);
+    if (e) {
+        DCX_CUDA(cudaMemsetAsync(c.d_err, 0, 4, c.stream));
+        if (e & DEV_ERR_TIMEOUT) throw Error(DCX_ERR_TIMEOUT, "a bounded device wait gave up");
+        throw Error(DCX_ERR_INTERNAL, "device range check failed");
+    }
+}
+
+// Device-wide exclusive scan with operator Op; returns the grand total.
+template <typename T, typename Op>
+static T device_scan(Ctx& c, const Op& op, uint64_t n) {
+    if (n == 0) return T(0);
+    const uint64_t tiles = div_up(n, SCAN_TILE);
+    DBuf<T> sums(&c, tiles + 1);
+    k_scan_reduce<T, Op><<<(unsigned)tiles, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get());
+    k_scan_tile_sums<T><<<1, 1024, 0, c.stream>>>(sums.get(), tiles, sums.get() + tiles);
+    k_scan_apply<T, Op><<<(unsigned)tiles, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get());
+    DCX_CHECK_LAUNCH();
+    c.launched(3);
+    return d2h_scalar(c, sums.get() + tiles);
+}
+
+static const DcHost& get_dc(Ctx& c, uint32_t X) {
+    auto it = c.dc_host.find(X);
+    if (it != c.dc_host.end()) return it->second;
+    DcHost h;
+    if (!make_dc(X, h)) throw Error(DCX_ERR_ARG, "unsupported difference cover X=" + std::to_string(X));
+    DcDev dd{};
+    dd.X = X;
+    dd.D = h.D;
+    for (uint32_t i = 0; i < X; i++) dd.next_rank[i] = h.next_rank[i];
+    for (uint32_t i = 0; i < h.D; i++) dd.dc[i] = h.dc[i];
+    for (uint32_t i = 0; i < X; i++)
+        for (uint32_t j = 0; j < X; j++) {
+            const uint32_t* e = &h.cmp[((size_t)i * X + j) * 3];
+            dd.cmp[i * X + j] = (uint16_t)(e[1] | (e[2] << 8));
+        }
+    DcDev* p = nullptr;
+    DCX_CUDA(cudaMalloc(&p, sizeof(DcDev)));
+    DCX_CUDA(cudaMemcpy(p, &dd, sizeof(DcDev), cudaMemcpyHostToDevice));
+    c.dc_dev[X] = p;
+    return c.dc_host.emplace(X, std::move(h)).first->second;
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort driver.  Keys/values in buffer 0, digit histograms of all 4*kw
+// passes in c.d_hist.  Passes whose digit is constant are skipped.  Returns the
+// index (0/1) of the buffer holding the sorted data.
+// ---------------------------------------------------------------------------
+struct SortSpace {
+    uint32_t* k[2][MAX_KEY_WORDS] = {};
+    uint32_t* v[2] = {};
+};
+
+static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
+    const uint32_t passes = 4 * kw;
+    std::vector<uint32_t> h((size_t)passes * RADIX);
+    DCX_CUDA(cudaMemcpyAsync(h.data(), c.d_hist, h.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<uint32_t> run;
+    std::vector<uint32_t> bases;
+    for (uint32_t p = 0; p < passes; p++) {
+        const uint32_t* hp = &h[(size_t)p * RADIX];
+        uint32_t mx = *std::max_element(hp, hp + RADIX);
+        if ((uint64_t)mx == count) continue;
+        run.push_back(p);
+        uint32_t acc = 0;
+        for (int d = 0; d < RADIX; d++) {
+            bases.push_back(acc);
+            acc += hp[d];
+        }
+    }
+    if (run.empty()) return 0;
+    constexpr int ITEMS = 16;
+    constexpr int TILE = SORT_THREADS * ITEMS;
+    const uint64_t tiles = div_up(count, TILE);
+    if (tiles > c.lookback_tiles) {
+        if (c.d_lookback) DCX_CUDA(cudaFree(c.d_lookback));
+        c.d_lookback = nullptr;
+        size_t want = std::max<size_t>(tiles, 1024);
+        DCX_CUDA(cudaMalloc(&c.d_lookback, want * RADIX * sizeof(uint64_t)));
+        DCX_CUDA(cudaMemset(c.d_lookback, 0, want * RADIX * sizeof(uint64_t)));
+        c.lookback_tiles = want;
+        c.epoch = 0;
+    }
+    DCX_CUDA(cudaMemcpyAsync(c.d_base, bases.data(), bases.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    DCX_CUDA(cudaMemsetAsync(c.d_tiles, 0, run.size() * 4, c.stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c.stream);
+    int cur = 0;
+    for (size_t i = 0; i < run.size(); i++) {
+        if (++c.epoch >= (1u << 30)) {
+            DCX_CUDA(cudaMemsetAsync(c.d_lookback, 0, c.lookback_tiles * RADIX * sizeof(uint64_t), c.stream));
+            c.epoch = 1;
+        }
+        SortPassArgs a{};
+        for (uint32_t w = 0; w < kw; w++) {
+            a.keys_in[w] = s.k[cur][w];
+            a.keys_out[w] = s.k[cur ^ 1][w];
+        }
+        a.vals_in = s.v[cur];
+        a.vals_out = s.v[cur ^ 1];
+        a.kw = kw;
+        a.n = count;
+        a.shift = run[i] * RADIX_BITS;
+        a.digit_base = c.d_base + i * RADIX;
+        a.lookback = c.d_lookback;
+        a.tile_counter = c.d_tiles + i;
+        a.epoch = c.epoch;
+        a.err = c.d_err;
+        a.spin_limit = c.opt.spin_limit;
+        k_onesweep<ITEMS><<<(unsigned)tiles, SORT_THREADS, 0, c.stream>>>(a);
+        DCX_CHECK_LAUNCH();
+        cur ^= 1;
+    }
+    cudaEventRecord(e1, c.stream);
+    DCX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.st.ms_radix += ms;
+    c.launched(run.size());
+    c.st.radix_passes += run.size();
+    c.st.radix_keys += run.size() * count;
+    const uint64_t b = (uint64_t)run.size() * count * (kw + 1) * 4 * 2;
+    c.st.bytes_radix += b;
+    c.alg(b);
+    return cur;
+}
+
+// ---------------------------------------------------------------------------
+// Phase 1: sort all N = n+1 suffixes by their first L chars.  Produces the
+// sorted positions `sa` and head flags (1 where the window differs from the
+// previous one).
+// ---------------------------------------------------------------------------
+template <typename CharT>
+static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint32_t L, int depth,
+                         DBuf<uint32_t>& sa, DBuf<uint8_t>& head) {
+    const uint64_t N = n + 1;
+    const uint32_t words_full = (key_bits(B, L) + 31) / 32;
+    uint32_t kw0_max = depth == 0 ? 2 : 3;
+    uint32_t P0 = std::min<uint32_t>(L, max_chars_in(B, std::min(words_full, kw0_max)));
+    if (c.opt.prefix_chars && depth == 0) P0 = std::min<uint32_t>(L, c.opt.prefix_chars);
+    if (P0 == 0) P0 = 1;
+    KeyPlan plan = make_plan(B, P0);
+    if (plan.kw > 3) throw Error(DCX_ERR_INTERNAL, "prefix key wider than 3 words");
+    const uint32_t kw = plan.kw;
+
+    // round 0
+    {
+        DBuf<uint32_t> keys[2][3];
+        DBuf<uint32_t> vals[2];
+        SortSpace s;
+        for (int b = 0; b < 2; b++) {
+            for (uint32_t w = 0; w < kw; w++) {
+                keys[b][w] = DBuf<uint32_t>(&c, N);
+                s.k[b][w] = keys[b][w].get();
+            }
+            vals[b] = DBuf<uint32_t>(&c, N);
+            s.v[b] = vals[b].get();
+        }
+        DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+        KeyOut ko{};
+        for (uint32_t w = 0; w < kw; w++) ko.w[w] = s.k[0][w];
+        const int grid = grid_for(N, 256, 148 * 8);
+        const size_t shm = 4 * kw * RADIX * 4;
+        if (kw == 1) k_keys_prefix<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
+        else if (kw == 2) k_keys_prefix<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
+        else k_keys_prefix<3, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(N * sizeof(CharT) + N * (kw + 1) * 4);
+        int f = radix_sort(c, kw, N, s);
+        KeyWords kk{};
+        for (uint32_t w = 0; w < kw; w++) kk.w[w] = s.k[f][w];
+        head = DBuf<uint8_t>(&c, N);
+        k_heads<<<grid_for(N, 256), 256, 0, c.stream>>>(kk, kw, N, head.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(N * kw * 4 + N);
+        sa = std::move(vals[f]);
+    }
+
+    // refinement rounds for tied windows
+    uint32_t covered = P0;
+    while (covered < L) {
+        DBuf<uint32_t> slot(&c, N), grp(&c, N);
+        OpTied op{head.get(), N, slot.get(), grp.get()};
+        const uint64_t tot = device_scan<uint64_t>(c, op, N);
+        c.alg(N + N / 2);
+        const uint64_t cnt = tot >> 32;
+        if (cnt == 0) break;
+        const uint32_t Pr = std::min<uint32_t>(L - covered, max_chars_in(B, 2));
+        KeyPlan rp = make_plan(B, Pr);
+        const uint32_t kwr = rp.kw + 1;  // + group number
+        DBuf<uint32_t> keys[2][3];
+        DBuf<uint32_t> vals[2];
+        SortSpace s;
+        for (int b = 0; b < 2; b++) {
+            for (uint32_t w = 0; w < kwr; w++) {
+                keys[b][w] = DBuf<uint32_t>(&c, cnt);
+                s.k[b][w] = keys[b][w].get();
+            }
+            vals[b] = DBuf<uint32_t>(&c, cnt);
+            s.v[b] = vals[b].get();
+        }
+        DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+        KeyOut ko{};
+        for (uint32_t w = 0; w < kwr; w++) ko.w[w] = s.k[0][w];
+        const int grid = grid_for(cnt, 256, 148 * 8);
+        const size_t shm = 4 * kwr * RADIX * 4;
+        if (rp.kw == 1)
+            k_keys_refine<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, slot.get(), grp.get(), sa.get(),
+                                                                  covered, rp, ko, s.v[0], c.d_hist);
+        else
+            k_keys_refine<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, slot.get(), grp.get(), sa.get(),
+                                                                  covered, rp, ko, s.v[0], c.d_hist);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(cnt * (12 + Pr * sizeof(CharT)) + cnt * (kwr + 1) * 4);
+        int f = radix_sort(c, kwr, cnt, s);
+        KeyWords kk{};
+        for (uint32_t w = 0; w < kwr; w++) kk.w[w] = s.k[f][w];
+        k_refine_scatter<<<grid_for(cnt, 256), 256, 0, c.stream>>>(cnt, slot.get(), kk, kwr, s.v[f], sa.get(),
+                                                                   head.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(cnt * (4 + kwr * 4 * 2 + 4 + 4 + 1));
+        covered += Pr;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase 4: order every tie group (equal L-char windows) by cover ranks.
+// ---------------------------------------------------------------------------
+template <int D>
+static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_text, const DcDev* dcd,
+                        const std::vector<uint32_t>& counts, const uint32_t* gstart, const uint32_t* gsize) {
+    std::vector<uint64_t> off(TIE_CLASSES + 1, 0);
+    for (int k = 0; k < TIE_CLASSES; k++) off[k + 1] = off[k] + counts[k];
+    auto warp_launch = [&](int cls, auto W) {
+        constexpr int Wv = decltype(W)::value;
+        const uint64_t g = counts[cls];
+        if (!g) return;
+        const uint64_t warps = div_up(g, 32 / Wv);
+        const uint64_t blocks = div_up(warps * 32, 256);
+        k_tie_warp<D, Wv><<<(unsigned)blocks, 256, 0, c.stream>>>(gstart + off[cls], gsize + off[cls], (uint32_t)g,
+                                                                  sa, rank_text, dcd);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    };
+    warp_launch(0, std::integral_constant<int, 2>{});
+    warp_launch(1, std::integral_constant<int, 4>{});
+    warp_launch(2, std::integral_constant<int, 8>{});
+    warp_launch(3, std::integral_constant<int, 16>{});
+    warp_launch(4, std::integral_constant<int, 32>{});
+    auto cta_launch = [&](int cls, const uint32_t* gs, const uint32_t* gz, uint64_t g, auto Cc) {
+        constexpr int C = decltype(Cc)::value;
+        constexpr int T = C / 2 < 512 ? C / 2 : 512;
+        if (!g) return;
+        const size_t shm = tie_cta_smem<D, C>();
+        DCX_CUDA(cudaFuncSetAttribute(k_tie_cta<D, C, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        for (uint64_t b = 0; b < g; b += 65535ull * 1024) {
+            const uint64_t nb = std::min<uint64_t>(g - b, 65535ull * 1024);
+            k_tie_cta<D, C, T><<<(unsigned)nb, T, shm, c.stream>>>(gs + b, gz + b, sa, rank_text, dcd);
+            DCX_CHECK_LAUNCH();
+            c.launched();
+        }
+        (void)cls;
+    };
+    cta_launch(5, gstart + off[5], gsize + off[5], counts[5], std::integral_constant<int, 64>{});
+    cta_launch(6, gstart + off[6], gsize + off[6], counts[6], std::integral_constant<int, 128>{});
+    cta_launch(7, gstart + off[7], gsize + off[7], counts[7], std::integral_constant<int, 256>{});
+    cta_launch(8, gstart + off[8], gsize + off[8], counts[8], std::integral_constant<int, 512>{});
+    cta_launch(9, gstart + off[9], gsize + off[9], counts[9], std::integral_constant<int, 1024>{});
+    cta_launch(10, gstart + off[10], gsize + off[10], counts[10], std::integral_constant<int, 2048>{});
+    const uint64_t nbig = counts[11];
+    if (!nbig) return;
+    // big groups: sort 2048-chunks, then merge rounds
+    std::vector<uint32_t> bstart(nbig), bsize(nbig);
+    DCX_CUDA(cudaMemcpyAsync(bstart.data(), gstart + off[11], nbig * 4, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaMemcpyAsync(bsize.data(), gsize + off[11], nbig * 4, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<uint32_t> cstart, csize;
+    std::vector<uint64_t> offs(nbig + 1, 0);
+    uint32_t maxsz = 0;
+    for (uint64_t g = 0; g < nbig; g++) {
+        for (uint32_t o = 0; o < bsize[g]; o += 2048) {
+            cstart.push_back(bstart[g] + o);
+            csize.push_back(std::min<uint32_t>(2048, bsize[g] - o));
+        }
+        offs[g + 1] = offs[g] + bsize[g];
+        maxsz = std::max(maxsz, bsize[g]);
+    }
+    DBuf<uint32_t> dcs(&c, cstart.size()), dcz(&c, csize.size()), dbs(&c, nbig);
+    DBuf<uint64_t> doff(&c, nbig + 1);
+    DCX_CUDA(cudaMemcpyAsync(dcs.get(), cstart.data(), cstart.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    DCX_CUDA(cudaMemcpyAsync(dcz.get(), csize.data(), csize.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    DCX_CUDA(cudaMemcpyAsync(dbs.get(), bstart.data(), nbig * 4, cudaMemcpyHostToDevice, c.stream));
+    DCX_CUDA(cudaMemcpyAsync(doff.get(), offs.data(), (nbig + 1) * 8, cudaMemcpyHostToDevice, c.stream));
+    cta_launch(11, dcs.get(), dcz.get(), cstart.size(), std::integral_constant<int, 2048>{});
+    DBuf<uint32_t> tmp(&c, N);
+    uint32_t* src = sa;
+    uint32_t* dst = tmp.get();
+    const uint64_t total = offs[nbig];
+    for (uint64_t w = 2048; w < maxsz; w <<= 1) {
+        k_tie_merge<D><<<grid_for(total, 256), 256, 0, c.stream>>>(doff.get(), (uint32_t)nbig, dbs.get(), total,
+                                                                   (uint32_t)w, src, dst, rank_text, dcd);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        std::swap(src, dst);
+    }
+    if (src != sa) {
+        k_copy_ranges<<<grid_for(total, 256), 256, 0, c.stream>>>(doff.get(), (uint32_t)nbig, dbs.get(), total, src, sa);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    }
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, const uint32_t* rank_text,
+                      const DcHost& dc) {
+    DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1);
+    OpGroups op{head, N, starts.get(), ends.get()};
+    const uint64_t tot = device_scan<uint64_t>(c, op, N);
+    c.alg(N);
+    const uint64_t G = tot & 0xffffffffull;
+    if (G == 0) return;
+    DBuf<uint32_t> cnt(&c, 2 * TIE_CLASSES);
+    DCX_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * TIE_CLASSES * 4, c.stream));
+    k_tie_classify<<<grid_for(G, 256), 256, 0, c.stream>>>(G, starts.get(), ends.get(), cnt.get());
+    DCX_CHECK_LAUNCH();
+    std::vector<uint32_t> counts(TIE_CLASSES);
+    DCX_CUDA(cudaMemcpyAsync(counts.data(), cnt.get(), TIE_CLASSES * 4, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<uint32_t> cursor(TIE_CLASSES, 0);
+    uint64_t acc = 0;
+    for (int k = 0; k < TIE_CLASSES; k++) {
+        cursor[k] = (uint32_t)acc;
+        acc += counts[k];
+    }
+    DCX_CUDA(cudaMemcpyAsync(cnt.get() + TIE_CLASSES, cursor.data(), TIE_CLASSES * 4, cudaMemcpyHostToDevice, c.stream));
+    DBuf<uint32_t> gstart(&c, G), gsize(&c, G);
+    k_tie_bin<<<grid_for(G, 256), 256, 0, c.stream>>>(G, starts.get(), ends.get(), cnt.get() + TIE_CLASSES,
+                                                       gstart.get(), gsize.get());
+    DCX_CHECK_LAUNCH();
+    c.launched(2);
+    starts.reset();
+    ends.reset();
+    const DcDev* dcd = c.dc_dev[dc.X];
+    switch (dc.D) {
+        case 2: tie_break_d<2>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 3: tie_break_d<3>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 4: tie_break_d<4>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 5: tie_break_d<5>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 6: tie_break_d<6>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 7: tie_break_d<7>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 8: tie_break_d<8>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 9: tie_break_d<9>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 10: tie_break_d<10>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 11: tie_break_d<11>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        case 12: tie_break_d<12>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+        default: throw Error(DCX_ERR_INTERNAL, "unsupported D");
+    }
+    c.st.tie_groups += G;
+}
+
+// ---------------------------------------------------------------------------
+// One DCX level.  text: device chars in 1..sigma, length n.  sa_out: n entries.
+// ---------------------------------------------------------------------------
+struct LevelInfo {
+    uint32_t sample_chars;
+};
+
+template <typename CharT>
+static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_t X, int depth, bool packing,
+                  uint32_t* sa_out);
+
+static void small_sa_single(Ctx& c, const void* text, bool wide, uint64_t n, uint32_t* sa_out) {
+    uint64_t offs[2] = {0, n};
+    DBuf<uint64_t> d(&c, 2);
+    DCX_CUDA(cudaMemcpyAsync(d.get(), offs, 16, cudaMemcpyHostToDevice, c.stream));
+    if (wide)
+        k_small_sa<uint32_t><<<1, SMALL_THREADS, 0, c.stream>>>((const uint32_t*)text, d.get(), nullptr, sa_out);
+    else
+        k_small_sa<uint8_t><<<1, SMALL_THREADS, 0, c.stream>>>((const uint8_t*)text, d.get(), nullptr, sa_out);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+static uint32_t level0_sample_chars(uint32_t X, uint64_t sigma, bool packing) {
+    if (!packing) return X;
+    // cli.cpp:488-533: 3 bits if sigma <= 7, 5 if <= 31, else 8; K = ceil(X / chars_per_word);
+    // the sample window is X * (K*cpw/X) chars computed in double (sample_string.hpp:131-133).
+    const uint32_t bits = sigma <= 7 ? 3 : (sigma <= 31 ? 5 : 8);
+    const uint32_t cpw = 64 / bits;
+    const uint32_t K = (X + cpw - 1) / cpw;
+    const double ratio = (double)(K * cpw) / X;
+    return (uint32_t)(X * ratio);
+}
+
+template <typename CharT>
+static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_t X, int depth, bool packing,
+                  uint32_t* sa_out) {
+    if (n == 0) return;
+    if (depth > 64) throw Error(DCX_ERR_INTERNAL, "recursion deeper than 64 levels");
+    c.st.levels = std::max<uint32_t>(c.st.levels, (uint32_t)depth + 1);
+    if (n <= c.opt.small_threshold && n <= (uint64_t)SMALL_MAX) {
+        small_sa_single(c, text, sizeof(CharT) == 4, n, sa_out);
+        return;
+    }
+    const DcHost& dc = get_dc(c, X);
+    const uint32_t D = dc.D;
+    const uint32_t L = depth == 0 ? level0_sample_chars(X, sigma, packing) : X;
+    const uint64_t B = sigma + 1;
+    const uint64_t N = n + 1;
+    const uint64_t rem = n % X;
+    const bool dummy = dc.in_dc[rem] != 0;
+    uint64_t m = (n / X) * D;
+    for (uint64_t r = 0; r < rem; r++) m += dc.in_dc[r];
+    m += dummy;
+    DcFlags fl{};
+    fl.X = X;
+    fl.D = D;
+    for (uint32_t i = 0; i < X; i++) {
+        fl.in_dc[i] = dc.in_dc[i];
+        fl.next_rank[i] = dc.next_rank[i];
+    }
+    for (uint32_t i = 0; i < D; i++) fl.dc[i] = dc.dc[i];
+    {
+        std::vector<uint64_t> num_at_mod(X);
+        for (uint64_t i = 0; i < X; i++) num_at_mod[i] = (n + X - 1 - i) / X;
+        num_at_mod[rem] += dummy;
+        fl.samples_before[0] = 0;
+        for (uint32_t i = 1; i <= D; i++) fl.samples_before[i] = fl.samples_before[i - 1] + num_at_mod[dc.dc[i - 1]];
+    }
+    DBuf<DcFlags> dfl(&c, 1);
+    DCX_CUDA(cudaMemcpyAsync(dfl.get(), &fl, sizeof(fl), cudaMemcpyHostToDevice, c.stream));
+
+    cudaEvent_t ev[5];
+    for (auto& e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[0], c.stream);
+
+    // ---- phase 1: window sort
+    DBuf<uint32_t> sa;
+    DBuf<uint8_t> head;
+    sort_windows<CharT>(c, text, n, B, L, depth, sa, head);
+
+    // ---- phase 2: names
+    DBuf<uint32_t> s_pos(&c, m), s_grp(&c, m);
+    {
+        OpSamples op{head.get(), sa.get(), dfl.get(), s_pos.get(), s_grp.get(), m};
+        const uint64_t tot = device_scan<uint64_t>(c, op, N);
+        c.alg(N * 5 + m * 8);
+        if ((tot >> 32) != m) throw Error(DCX_ERR_INTERNAL, "sample count mismatch");
+    }
+    DBuf<uint32_t> name(&c, m);
+    DBuf<uint8_t> uniq(&c, m);
+    {
+        OpNames op{s_grp.get(), m, name.get(), uniq.get()};
+        device_scan<uint32_t>(c, op, m);
+        c.alg(m * 9);
+    }
+    s_grp.reset();
+    const uint32_t last_rank = d2h_scalar(c, name.get() + (m - 1));
+    if (depth == 0) {
+        c.st.level0_samples = m;
+        c.st.level0_last_rank = last_rank;
+        c.st.level0_recursion = 0;
+        c.st.level0_reduction = 0;
+        if (c.opt.trace) {
+            DBuf<uint32_t> tn(&c, m);
+            DBuf<uint8_t> tu(&c, m);
+            k_scatter_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), dfl.get(), nullptr,
+                                                                   tn.get(), tu.get(), uniq.get());
+            DCX_CHECK_LAUNCH();
+            c.trace_names.resize(m);
+            c.trace_uniq.resize(m);
+            DCX_CUDA(cudaMemcpyAsync(c.trace_names.data(), tn.get(), m * 4, cudaMemcpyDeviceToHost, c.stream));
+            DCX_CUDA(cudaMemcpyAsync(c.trace_uniq.data(), tu.get(), m, cudaMemcpyDeviceToHost, c.stream));
+            DCX_CUDA(cudaStreamSynchronize(c.stream));
+        }
+    }
+    cudaEventRecord(ev[1], c.stream);
+
+    // ---- phase 3: ranks of the samples (sample text order, D zero slots of padding)
+    DBuf<uint32_t> rank_text(&c, m + D);
+    DCX_CUDA(cudaMemsetAsync(rank_text.get(), 0, (m + D) * 4, c.stream));
+    if (last_rank >= m) {
+        k_scatter_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), dfl.get(), rank_text.get(),
+                                                               nullptr, nullptr, nullptr);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(m * 12);
+    } else {
+        const uint32_t Xr = c.opt.recursion_dc ? c.opt.recursion_dc : X;
+        DBuf<uint32_t> rec(&c, m), q_of_j(&c, m);
+        DBuf<uint8_t> rec_uniq(&c, m);
+        k_build_rec<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), uniq.get(), dfl.get(),
+                                                           rec.get(), rec_uniq.get(), q_of_j.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(m * 21);
+        // discarding decision (pdcx.hpp:150-165)
+        DBuf<uint32_t> kidx(&c, m);
+        OpKeep kop{rec_uniq.get(), rec.get(), nullptr, kidx.get()};
+        const uint32_t after = device_scan<uint32_t>(c, kop, m);
+        c.alg(m * 6);
+        const double reduction = (double)after / (double)m;
+        const bool discard = reduction <= c.opt.discarding_threshold;
+        if (depth == 0) {
+            c.st.level0_recursion = discard ? 2 : 1;
+            c.st.level0_reduction = reduction;
+        }
+        if (!discard) {
+            kidx.reset();
+            q_of_j.reset();
+            rec_uniq.reset();
+            DBuf<uint32_t> sa_r(&c, m);
+            level<uint32_t>(c, rec.get(), m, last_rank, Xr, depth + 1, false, sa_r.get());
+            rec.reset();
+            k_ranks_from_rec<<<grid_for(m, 256), 256, 0, c.stream>>>(m, sa_r.get(), dfl.get(), rank_text.get());
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            c.alg(m * 8);
+        } else {
+            DBuf<uint32_t> rec2(&c, after);
+            OpKeep kop2{rec_uniq.get(), rec.get(), rec2.get(), nullptr};
+            device_scan<uint32_t>(c, kop2, m);
+            c.alg(m * 6 + after * 4);
+            rec.reset();
+            rec_uniq.reset();
+            DBuf<uint32_t> sa2(&c, after);
+            level<uint32_t>(c, rec2.get(), after, last_rank, Xr, depth + 1, false, sa2.get());
+            rec2.reset();
+            DBuf<uint32_t> rank_of(&c, after);
+            k_inverse<<<grid_for(after, 256), 256, 0, c.stream>>>(after, sa2.get(), rank_of.get());
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            sa2.reset();
+            // non-unique samples keyed by (name, rank2)
+            DBuf<uint32_t> keys[2][2];
+            DBuf<uint32_t> vals[2];
+            SortSpace s;
+            for (int b = 0; b < 2; b++) {
+                for (int w = 0; w < 2; w++) {
+                    keys[b][w] = DBuf<uint32_t>(&c, m);
+                    s.k[b][w] = keys[b][w].get();
+                }
+                vals[b] = DBuf<uint32_t>(&c, m);
+                s.v[b] = vals[b].get();
+            }
+            OpNonUnique nop{uniq.get(), name.get(), q_of_j.get(), kidx.get(), rank_of.get(), s.k[0][0], s.k[0][1],
+                            s.v[0]};
+            const uint32_t mu = device_scan<uint32_t>(c, nop, m);
+            c.alg(m + mu * 24);
+            rank_of.reset();
+            kidx.reset();
+            q_of_j.reset();
+            if (mu) {
+                DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+                SortPassArgs ha{};
+                ha.keys_in[0] = s.k[0][0];
+                ha.keys_in[1] = s.k[0][1];
+                ha.kw = 2;
+                ha.n = mu;
+                k_digit_hist<<<grid_for(mu, 256, 148 * 4), 256, 8 * RADIX * 4, c.stream>>>(ha, c.d_hist);
+                DCX_CHECK_LAUNCH();
+                c.launched();
+                c.alg(mu * 8);
+                int f = radix_sort(c, 2, mu, s);
+                DBuf<uint32_t> start_s(&c, (uint64_t)last_rank + 1), start_l(&c, (uint64_t)last_rank + 1);
+                k_name_starts<<<grid_for(m, 256), 256, 0, c.stream>>>(m, name.get(), start_s.get());
+                k_name_starts<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], start_l.get());
+                k_ranks_after_discarding<<<grid_for(mu, 256), 256, 0, c.stream>>>(
+                    mu, s.k[f][1], s.v[f], start_s.get(), start_l.get(), s_pos.get(), dfl.get(), rank_text.get());
+                DCX_CHECK_LAUNCH();
+                c.launched(3);
+                c.alg(m * 8 + mu * 8 + mu * 24);
+            }
+            k_ranks_unique<<<grid_for(m, 256), 256, 0, c.stream>>>(m, uniq.get(), s_pos.get(), dfl.get(),
+                                                                  rank_text.get());
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            c.alg(m * 9);
+        }
+    }
+    s_pos.reset();
+    name.reset();
+    uniq.reset();
+    cudaEventRecord(ev[2], c.stream);
+
+    // ---- phase 4: tie groups, then emit
+    tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc);
+    head.reset();
+    rank_text.reset();
+    k_emit32<<<grid_for(n, 256), 256, 0, c.stream>>>(sa.get(), n, sa_out);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    c.alg(n * 8);
+    cudaEventRecord(ev[3], c.stream);
+    DCX_CUDA(cudaEventSynchronize(ev[3]));
+    if (depth == 0) {
+        float a = 0, b = 0, d = 0;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        cudaEventElapsedTime(&d, ev[2], ev[3]);
+        c.st.ms_phase12 += a;
+        c.st.ms_phase3 += b;
+        c.st.ms_phase4 += d;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    check_device_error(c);
+}
+
+// ---------------------------------------------------------------------------
+// Whole build for one text (device or host pointers).
+// ---------------------------------------------------------------------------
+static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width, void* sa_out, uint32_t flags,
+                      bool strict) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (n && (!text || !sa_out)) throw Error(DCX_ERR_ARG, "null pointer");
+    get_dc(c, (uint32_t)X);
+    c.st = dcx_stats{};
+    c.peak = c.in_use;
+    if (n == 0) return;
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    const bool packing = !(flags & DCX_NO_PACKING);
+    cudaEvent_t e0, e1, e2, e3;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventCreate(&e3);
+    cudaEventRecord(e0, c.stream);
+    DBuf<uint8_t> t_in;
+    const uint8_t* dtext = text;
+    if (dev && ((uintptr_t)text & 15)) {  // the byte kernels load 16 bytes at a time
+        t_in = DBuf<uint8_t>(&c, n + 16);
+        DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyDeviceToDevice, c.stream));
+        dtext = t_in.get();
+    } else if (!dev) {
+        t_in = DBuf<uint8_t>(&c, n + 16);
+        DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyHostToDevice, c.stream));
+        dtext = t_in.get();
+    }
+    cudaEventRecord(e1, c.stream);
+    // phase 0: alphabet (compress_alphabet, cli.cpp:417-463)
+    DBuf<uint8_t> t_map(&c, n + 16);
+    uint64_t sigma = 0;
+    bool wide_text = false;
+    if (flags & DCX_NO_REMAP) {
+        DCX_CUDA(cudaMemcpyAsync(t_map.get(), dtext, n, cudaMemcpyDeviceToDevice, c.stream));
+        DCX_CUDA(cudaMemsetAsync(c.d_h256, 0, 256 * 8, c.stream));
+        k_hist256<<<grid_for(n / 16 + 1, 256, 148 * 4), 256, 0, c.stream>>>(t_map.get(), n, c.d_h256);
+        DCX_CHECK_LAUNCH();
+        unsigned long long h[256];
+        DCX_CUDA(cudaMemcpyAsync(h, c.d_h256, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        DCX_CUDA(cudaStreamSynchronize(c.stream));
+        if (h[0]) throw Error(DCX_ERR_ARG, "char 0 is reserved for padding");
+        for (int i = 255; i > 0; i--)
+            if (h[i]) {
+                sigma = i;
+                break;
+            }
+    } else {
+        DCX_CUDA(cudaMemsetAsync(c.d_h256, 0, 256 * 8, c.stream));
+        k_hist256<<<grid_for(n / 16 + 1, 256, 148 * 4), 256, 0, c.stream>>>(dtext, n, c.d_h256);
+        DCX_CHECK_LAUNCH();
+        unsigned long long h[256];
+        DCX_CUDA(cudaMemcpyAsync(h, c.d_h256, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        DCX_CUDA(cudaStreamSynchronize(c.stream));
+        ByteMap map{};
+        uint32_t next = 1;
+        for (int i = 0; i < 256; i++)
+            if (h[i]) map.m[i] = (uint8_t)(next++);
+        sigma = next - 1;
+        if (sigma == 256 && strict)
+            throw Error(DCX_ERR_ALPHABET, "256 distinct symbols: 0 is reserved for padding");
+        if (sigma == 256) wide_text = true;  // chars 1..256 need 32-bit storage
+        else k_remap<<<grid_for(n / 16 + 1, 256, 148 * 8), 256, 0, c.stream>>>(dtext, t_map.get(), n, map);
+        DCX_CHECK_LAUNCH();
+    }
+    c.launched(2);
+    c.alg(n * 3);
+    c.st.sigma = (uint32_t)sigma;
+    cudaEventRecord(e2, c.stream);
+    DBuf<uint32_t> sa32;
+    uint32_t* out32 = nullptr;
+    if (dev && width == 32) {
+        out32 = (uint32_t*)sa_out;
+    } else {
+        sa32 = DBuf<uint32_t>(&c, n);
+        out32 = sa32.get();
+    }
+    if (wide_text) {
+        // all 256 byte values occur: remap b -> b + 1 into 32-bit chars and build
+        // with 257-symbol keys (the reference cli refuses this input)
+        DBuf<uint32_t> t32(&c, n);
+        k_widen_text<<<grid_for(n, 256), 256, 0, c.stream>>>(dtext, n, t32.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        t_in.reset();
+        t_map.reset();
+        level<uint32_t>(c, t32.get(), n, sigma, (uint32_t)X, 0, packing, out32);
+    } else {
+        t_in.reset();
+        level<uint8_t>(c, t_map.get(), n, sigma, (uint32_t)X, 0, packing, out32);
+    }
+    t_map.reset();
+    DBuf<uint8_t> wide;
+    if (width != 32) {
+        uint8_t* wout = dev ? (uint8_t*)sa_out : nullptr;
+        if (!dev) {
+            wide = DBuf<uint8_t>(&c, n * (width / 8));
+            wout = wide.get();
+        }
+        k_widen<<<grid_for(n, 256), 256, 0, c.stream>>>(out32, n, wout, width);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(n * (4 + width / 8));
+    }
+    cudaEventRecord(e3, c.stream);
+    if (!dev) {
+        const void* src = width == 32 ? (const void*)out32 : (const void*)wide.get();
+        DCX_CUDA(cudaMemcpyAsync(sa_out, src, n * (width / 8), cudaMemcpyDeviceToHost, c.stream));
+    }
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    float h2d = 0, p0 = 0, total = 0;
+    cudaEventElapsedTime(&h2d, e0, e1);
+    cudaEventElapsedTime(&p0, e1, e2);
+    cudaEventElapsedTime(&total, e1, e3);
+    c.st.ms_h2d = h2d;
+    c.st.ms_phase0 = p0;
+    c.st.ms_total = total;
+    c.st.peak_bytes = c.peak;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    cudaEventDestroy(e3);
+}
+
+}  // namespace dcx
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+struct dcx_ctx {
+    dcx::Ctx c;
+};
+
+using dcx::Error;
+
+template <typename F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return DCX_OK;
+    } catch (const Error& e) {
+        if (getenv("DCX_VERBOSE")) fprintf(stderr, "dcx: %s\n", e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        return DCX_ERR_OOM;
+    } catch (...) {
+        return DCX_ERR_INTERNAL;
+    }
+}
+
+extern "C" {
+
+const char* dcx_version(void) { return "dcx-b200 0.1"; }
+
+const char* dcx_strerror(int code) {
+    switch (code) {
+        case DCX_OK: return "ok";
+        case DCX_ERR_ARG: return "invalid argument";
+        case DCX_ERR_ALPHABET: return "alphabet of 256 symbols (0 is reserved for padding)";
+        case DCX_ERR_OOM: return "out of device memory";
+        case DCX_ERR_BUDGET: return "projected device footprint above the budget";
+        case DCX_ERR_TIMEOUT: return "bounded device wait gave up";
+        case DCX_ERR_CUDA: return "CUDA error";
+        case DCX_ERR_INTERNAL: return "internal error";
+        case DCX_ERR_BUSY: return "busy";
+        case DCX_ERR_NOTFOUND: return "unknown request";
+        default: return "unknown error";
+    }
+}
+
+int dcx_dc_table(int X, uint32_t* D, uint32_t* dc, uint32_t* next_rank, uint32_t* cmp) {
+    dcx::DcHost h;
+    if (X <= 0 || !dcx::make_dc((uint32_t)X, h)) return DCX_ERR_ARG;
+    if (D) *D = h.D;
+    if (dc) memcpy(dc, h.dc.data(), h.D * 4);
+    if (next_rank) memcpy(next_rank, h.next_rank.data(), X * 4);
+    if (cmp) memcpy(cmp, h.cmp.data(), h.cmp.size() * 4);
+    return DCX_OK;
+}
+
+int dcx_ctx_create(dcx_ctx** out, int device, uint64_t budget) {
+    if (!out) return DCX_ERR_ARG;
+    *out = nullptr;
+    return guarded([&] {
+        auto* x = new dcx_ctx();
+        dcx::Ctx& c = x->c;
+        try {
+            c.device = device;
+            DCX_CUDA(cudaSetDevice(device));
+            DCX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            cudaMemPool_t pool;
+            DCX_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+            uint64_t thr = UINT64_MAX;
+            DCX_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+            size_t fr = 0, tot = 0;
+            DCX_CUDA(cudaMemGetInfo(&fr, &tot));
+            c.budget = budget ? budget : (uint64_t)(fr * 0.9);
+            DCX_CUDA(cudaMalloc(&c.d_hist, 16 * dcx::RADIX * 4));
+            DCX_CUDA(cudaMalloc(&c.d_base, 16 * dcx::RADIX * 4));
+            DCX_CUDA(cudaMalloc(&c.d_tiles, 64 * 4));
+            DCX_CUDA(cudaMalloc(&c.d_err, 4));
+            DCX_CUDA(cudaMemset(c.d_err, 0, 4));
+            DCX_CUDA(cudaMalloc(&c.d_h256, 256 * 8));
+        } catch (...) {
+            delete x;
+            throw;
+        }
+        *out = x;
+    });
+}
+
+int dcx_ctx_destroy(dcx_ctx* x) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        dcx::Ctx& c = x->c;
+        cudaSetDevice(c.device);
+        if (c.stream) cudaStreamSynchronize(c.stream);
+        cudaFree(c.d_hist);
+        cudaFree(c.d_base);
+        cudaFree(c.d_tiles);
+        cudaFree(c.d_err);
+        cudaFree(c.d_h256);
+        if (c.d_lookback) cudaFree(c.d_lookback);
+        for (auto& kv : c.dc_dev) cudaFree(kv.second);
+        if (c.stream) cudaStreamDestroy(c.stream);
+        delete x;
+    });
+}
+
+int dcx_set_option(dcx_ctx* x, const char* name, double value) {
+    if (!x || !name) return DCX_ERR_ARG;
+    dcx::Options& o = x->c.opt;
+    std::string s(name);
+    if (s == "discarding_threshold") o.discarding_threshold = value;
+    else if (s == "recursion_dc") {
+        dcx::DcHost h;
+        if (value != 0 && !dcx::make_dc((uint32_t)value, h)) return DCX_ERR_ARG;
+        o.recursion_dc = (uint32_t)value;
+    } else if (s == "small_threshold") {
+        if (value < 0 || value > dcx::SMALL_MAX) return DCX_ERR_ARG;
+        o.small_threshold = (uint32_t)value;
+    } else if (s == "prefix_chars") o.prefix_chars = (uint32_t)value;
+    else if (s == "trace") o.trace = value != 0;
+    else if (s == "spin_limit") o.spin_limit = (uint32_t)value;
+    else return DCX_ERR_ARG;
+    return DCX_OK;
+}
+
+static int build_entry(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags,
+                       bool strict) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::build_one(x->c, text, n, dc, w, out, flags, strict);
+    });
+}
+
+int dcx_build_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags) {
+    return build_entry(x, text, n, dc, w, out, flags, false);
+}
+
+int dcx_build_sa_strict(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags) {
+    return build_entry(x, text, n, dc, w, out, flags, true);
+}
+
+int dcx_get_stats(dcx_ctx* x, dcx_stats* out) {
+    if (!x || !out) return DCX_ERR_ARG;
+    *out = x->c.st;
+    return DCX_OK;
+}
+
+int dcx_get_trace(dcx_ctx* x, uint64_t* m_out, uint32_t* names, uint8_t* unique, uint64_t cap) {
+    if (!x) return DCX_ERR_ARG;
+    const uint64_t m = x->c.trace_names.size();
+    if (m_out) *m_out = m;
+    if (names || unique) {
+        if (cap < m) return DCX_ERR_ARG;
+        if (names) memcpy(names, x->c.trace_names.data(), m * 4);
+        if (unique) memcpy(unique, x->c.trace_uniq.data(), m);
+    }
+    return DCX_OK;
+}
+
+int dcx_build_sa_batch(dcx_ctx*, const uint8_t*, const uint64_t*, uint32_t, int, int, void*, uint32_t) {
+    return DCX_ERR_INTERNAL;
+}
+int dcx_serve_submit(dcx_ctx*, const uint8_t*, uint64_t, int, int, uint64_t*) { return DCX_ERR_INTERNAL; }
+int dcx_serve_poll(dcx_ctx*, uint64_t, void*, int*, double*) { return DCX_ERR_INTERNAL; }
+int dcx_serve_release(dcx_ctx*, uint64_t) { return DCX_ERR_INTERNAL; }
+int dcx_serve_drain(dcx_ctx*) { return DCX_OK; }
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// Phase-4 tie breaking: orders the suffixes inside groups whose first L chars
+// are equal, with the difference-cover comparator of the reference
+// (DCMergeSamples::operator<, lightweight_dcx/src/pdcx/merge_samples.hpp:87-109,
+// and tie_break_ranks, merge_samples.hpp:262-306):
+//     (d, r1, r2) = cmpDepthRanks[i mod X][j mod X]
+//     i < j  <=>  ranks_i[r1] < ranks_j[r2]
+// where ranks_i are the D sample ranks starting at the first sample >= i
+// (get_global_ranks_pos, merge_samples.hpp:181-188).  The chars are already equal
+// for the whole window (L >= X > d), so only the rank comparison remains.
+//
+// Groups are binned by size: up to 32 elements are sorted by a bitonic network
+// inside W = 2..32 lanes of a warp (several groups per warp); up to 2048 by a
+// bitonic network in shared memory of one CTA; larger groups are cut into
+// 2048-chunks sorted the same way and then merged in rounds where every element
+// finds its output slot by binary search in the partner run.
+#pragma once
+
+#include "common.cuh"
+
+namespace dcx {
+
+constexpr int MAX_X = 133;
+constexpr int MAX_D = 12;
+constexpr uint32_t INVALID_POS = 0xffffffffu;
+
+struct DcDev {
+    uint32_t X, D;
+    uint32_t next_rank[MAX_X];
+    uint32_t dc[MAX_D];
+    uint16_t cmp[MAX_X * MAX_X];  // r1 | r2 << 8
+};
+
+template <int D>
+struct Rec {
+    uint32_t pos;
+    uint32_t r[D];
+};
+
+template <int D>
+__device__ __forceinline__ Rec<D> load_rec(uint32_t pos, const uint32_t* __restrict__ rank_text, uint32_t X,
+                                           const uint32_t* next_rank) {
+    Rec<D> r;
+    r.pos = pos;
+    if (pos == INVALID_POS) {
+#pragma unroll
+        for (int k = 0; k < D; k++) r.r[k] = 0;
+        return r;
+    }
+    const uint64_t rp = (uint64_t)(pos / X) * D + next_rank[pos % X];
+#pragma unroll
+    for (int k = 0; k < D; k++) r.r[k] = __ldg(rank_text + rp + k);
+    return r;
+}
+
+template <int D>
+__device__ __forceinline__ uint32_t pick(const Rec<D>& a, uint32_t k) {
+    uint32_t v = a.r[0];
+#pragma unroll
+    for (int t = 1; t < D; t++)
+        if (k == (uint32_t)t) v = a.r[t];
+    return v;
+}
+
+// a < b under the difference-cover comparator; invalid records sort last.
+template <int D>
+__device__ __forceinline__ bool dc_less(const Rec<D>& a, const Rec<D>& b, uint32_t X, const uint16_t* tab) {
+    if (a.pos == INVALID_POS) return false;
+    if (b.pos == INVALID_POS) return true;
+    const uint16_t e = tab[(a.pos % X) * X + (b.pos % X)];
+    return pick<D>(a, e & 0xffu) < pick<D>(b, e >> 8);
+}
+
+template <int D>
+__device__ __forceinline__ Rec<D> shfl_xor_rec(const Rec<D>& a, int j) {
+    Rec<D> o;
+    o.pos = __shfl_xor_sync(0xffffffffu, a.pos, j);
+#pragma unroll
+    for (int k = 0; k < D; k++) o.r[k] = __shfl_xor_sync(0xffffffffu, a.r[k], j);
+    return o;
+}
+
+__device__ __forceinline__ void load_dc_smem(const DcDev& dc, uint16_t* tab, uint32_t* nr) {
+    const uint32_t XX = dc.X * dc.X;
+    for (uint32_t i = threadIdx.x; i < XX; i += blockDim.x) tab[i] = dc.cmp[i];
+    for (uint32_t i = threadIdx.x; i < dc.X; i += blockDim.x) nr[i] = dc.next_rank[i];
+    __syncthreads();
+}
+
+// Groups of 2..W elements, 32/W groups per warp.
+template <int D, int W>
+__global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize,
+                                                  uint32_t ngroups, uint32_t* __restrict__ sa,
+                                                  const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp) {
+    __shared__ uint16_t tab[MAX_X * MAX_X];
+    __shared__ uint32_t nr[MAX_X];
+    load_dc_smem(*dcp, tab, nr);
+    const uint32_t X = dcp->X;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp_global = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t g = warp_global * (32 / W) + lane / W;
+    const uint32_t l = lane % W;
+    bool valid = false;
+    uint32_t start = 0;
+    if (g < ngroups) {
+        start = gstart[g];
+        valid = l < gsize[g];
+    }
+    Rec<D> a = load_rec<D>(valid ? sa[start + l] : INVALID_POS, rank_text, X, nr);
+#pragma unroll
+    for (int k = 2; k <= W; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            Rec<D> b = shfl_xor_rec<D>(a, j);
+            const bool up = (k == W) ? true : ((l & k) == 0);
+            const bool lower = (l & j) == 0;
+            // lower lane keeps the smaller element when sorting up
+            const bool b_less = dc_less<D>(b, a, X, tab);
+            const bool a_less = dc_less<D>(a, b, X, tab);
+            const bool take_b = (lower == up) ? b_less : a_less;
+            if (take_b) a = b;
+        }
+    }
+    if (valid) sa[start + l] = a.pos;
+}
+
+// One group (or chunk) of up to C elements per CTA; bitonic network in shared memory.
+template <int D, int C, int THREADS>
+__global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize,
+                                                     uint32_t* __restrict__ sa, const uint32_t* __restrict__ rank_text,
+                                                     const DcDev* __restrict__ dcp) {
+    extern __shared__ uint32_t smem[];
+    uint16_t* tab = reinterpret_cast<uint16_t*>(smem);
+    uint32_t* nr = smem + (MAX_X * MAX_X + 1) / 2;
+    Rec<D>* recs = reinterpret_cast<Rec<D>*>(nr + MAX_X);
+    load_dc_smem(*dcp, tab, nr);
+    const uint32_t X = dcp->X;
+    const uint32_t start = gstart[blockIdx.x], size = gsize[blockIdx.x];
+    for (uint32_t i = threadIdx.x; i < C; i += THREADS)
+        recs[i] = load_rec<D>(i < size ? sa[start + i] : INVALID_POS, rank_text, X, nr);
+    __syncthreads();
+    for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t p = threadIdx.x; p < (uint32_t)C / 2; p += THREADS) {
+                const uint32_t i = 2 * j * (p / j) + (p % j);
+                const uint32_t q = i + j;
+                const bool up = (i & k) == 0;
+                Rec<D> a = recs[i], b = recs[q];
+                const bool swap = up ? dc_less<D>(b, a, X, tab) : dc_less<D>(a, b, X, tab);
+                if (swap) {
+                    recs[i] = b;
+                    recs[q] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < size; i += THREADS) sa[start + i] = recs[i].pos;
+}
+
+template <int D, int C>
+constexpr size_t tie_cta_smem() {
+    return sizeof(uint32_t) * ((MAX_X * MAX_X + 1) / 2 + MAX_X) + sizeof(Rec<D>) * C;
+}
+
+// One merge round for groups larger than a chunk.  Flat element f belongs to
+// big group g (offsets[g] <= f < offsets[g+1]); runs of width w inside the group
+// are sorted; pairs of runs are merged from src into dst.
+template <int D>
+__global__ __launch_bounds__(256) void k_tie_merge(const uint64_t* __restrict__ offsets, uint32_t ngroups,
+                                                   const uint32_t* __restrict__ gstart, uint64_t total, uint32_t w,
+                                                   const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                                   const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp) {
+    __shared__ uint16_t tab[MAX_X * MAX_X];
+    __shared__ uint32_t nr[MAX_X];
+    load_dc_smem(*dcp, tab, nr);
+    const uint32_t X = dcp->X;
+    for (uint64_t f = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; f < total; f += (uint64_t)gridDim.x * blockDim.x) {
+        // group of f
+        uint32_t lo = 0, hi = ngroups;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= f) lo = mid; else hi = mid;
+        }
+        const uint32_t g = lo;
+        const uint64_t size = offsets[g + 1] - offsets[g];
+        const uint64_t o = f - offsets[g];
+        const uint64_t base = gstart[g];
+        const uint64_t run = o / w;
+        const uint64_t pair_base = (run & ~1ull) * w;
+        const bool left = (run & 1ull) == 0;
+        const uint64_t own_start = run * w;
+        uint64_t p_start, p_end;
+        if (left) {
+            p_start = own_start + w;
+            p_end = p_start + w < size ? p_start + w : size;
+        } else {
+            p_start = own_start - w;
+            p_end = own_start;
+        }
+        const Rec<D> me = load_rec<D>(src[base + o], rank_text, X, nr);
+        uint64_t a = p_start, b = p_end;  // count partner elements < me
+        if (p_start < size) {
+            while (a < b) {
+                uint64_t mid = (a + b) >> 1;
+                Rec<D> other = load_rec<D>(src[base + mid], rank_text, X, nr);
+                if (dc_less<D>(other, me, X, tab)) a = mid + 1; else b = mid;
+            }
+        } else {
+            a = p_start;
+        }
+        const uint64_t before = (p_start < size ? a - p_start : 0);
+        dst[base + pair_base + (o - own_start) + before] = me.pos;
+    }
+}
+
+}  // namespace dcx

@@ -1,0 +1,153 @@
+/*
+ * dcx_gpu.h -- C ABI of the B200 DCX suffix-array builder.
+ *
+ * The reference (lightweight_dcx of distributed_suffix_sorting_evaluation)
+ * exposes its construction path through two surfaces, and this ABI covers both:
+ *   - the library call  PDCX<char,index,DC>::compute_sa(std::vector<char>&)
+ *     -> std::vector<index>   (lightweight_dcx/src/pdcx/pdcx.hpp:529), wrapped
+ *     by run_pdcx / compute_sa (lightweight_dcx/src/executables/cli.cpp:465-472,655-689);
+ *   - the `cli` process (cli.cpp:747-820), rebuilt on top of this ABI as
+ *     `dcx_cli` with the same flags.
+ * Its error model follows libsais64 (libsais/include/libsais64.h:61): 0 on
+ * success, a negative code otherwise.  The library never exits the process and
+ * never falls back to the CPU.
+ *
+ * Threading: a context serves one host thread for dcx_build_* calls.
+ * dcx_serve_* calls are thread-safe (internal queue and worker thread).
+ * Ownership: callers own every buffer they pass; a context never retains a
+ * caller pointer beyond the call that received it.
+ */
+#ifndef DCX_GPU_H
+#define DCX_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define DCX_OK 0
+#define DCX_ERR_ARG (-1)      /* invalid argument (size, DC, width, null pointer) */
+#define DCX_ERR_ALPHABET (-2) /* 256 distinct byte values with packing requested (cli.cpp:440-446) */
+#define DCX_ERR_OOM (-3)      /* device allocation failed */
+#define DCX_ERR_BUDGET (-4)   /* projected HBM footprint above the context budget */
+#define DCX_ERR_TIMEOUT (-5)  /* a bounded device-side wait gave up (kernel returned cleanly) */
+#define DCX_ERR_CUDA (-6)     /* CUDA runtime error */
+#define DCX_ERR_INTERNAL (-7) /* internal consistency check failed */
+#define DCX_ERR_BUSY (-8)     /* serving queue full or request not finished */
+#define DCX_ERR_NOTFOUND (-9) /* unknown serving request id */
+
+/* ---- flags for dcx_build_sa / dcx_build_sa_batch ---------------------------- */
+#define DCX_HOST_PTRS 0u        /* text / sa_out are host pointers (pinned or pageable) */
+#define DCX_DEVICE_PTRS 1u      /* text / sa_out are device pointers on the context's GPU */
+#define DCX_NO_PACKING 2u       /* level-0 keys use X chars instead of the packed word width */
+#define DCX_NO_REMAP 4u         /* text is already remapped to 1..sigma (skip compress_alphabet) */
+
+/* SA output widths: 32 (uint32 LE), 40 (uint40 LE: low uint32 then high uint8,
+ * the reference's on-disk format, util/uint_types.hpp:49-269 + mpi/io.hpp:80-98),
+ * 64 (uint64 LE). */
+
+typedef struct dcx_ctx dcx_ctx;
+
+/* Per-build statistics (phase names follow pdcx.hpp:544,659,741,778). */
+typedef struct dcx_stats {
+    double ms_total;          /* device time of the whole build (CUDA events) */
+    double ms_phase0;         /* preparation: alphabet remap, key materialisation */
+    double ms_phase12;        /* phase 1 + 2: sample sort, naming */
+    double ms_phase3;         /* recursion */
+    double ms_phase4;         /* merge: tie-group sort and SA emission */
+    double ms_h2d;            /* host->device copies (host-pointer calls) */
+    double ms_d2h;            /* device->host copies (host-pointer calls) */
+    uint64_t bytes_alg;       /* algorithmic bytes of all kernels (read + write, logical) */
+    uint64_t bytes_radix;     /* algorithmic bytes of the radix-sort passes alone */
+    double ms_radix;          /* device time of the radix-sort passes alone */
+    uint64_t radix_passes;    /* radix passes executed (all levels) */
+    uint64_t radix_keys;      /* sum over passes of keys moved */
+    uint64_t kernel_launches; /* kernels launched by the build */
+    uint64_t peak_bytes;      /* device memory high-water mark of the build */
+    uint32_t levels;          /* recursion levels entered (1 = no recursion) */
+    uint32_t sigma;           /* alphabet size after remapping */
+    uint64_t level0_samples;  /* m at level 0 */
+    uint64_t level0_last_rank;/* highest level-0 name (== m iff all distinct) */
+    int level0_recursion;     /* 0 none, 1 direct, 2 discarding */
+    double level0_reduction;  /* discarding reduction at level 0 */
+    uint64_t tie_groups;      /* phase-4 tie groups (all levels) */
+    uint64_t tie_elements;    /* elements in phase-4 tie groups (all levels) */
+} dcx_stats;
+
+/* ---- context --------------------------------------------------------------- */
+/* Creates a context on `device` whose builds may hold at most hbm_budget_bytes
+ * of device memory (0 = 90% of the free memory at creation). */
+int dcx_ctx_create(dcx_ctx** out, int device, uint64_t hbm_budget_bytes);
+int dcx_ctx_destroy(dcx_ctx* ctx);
+
+/* Tuning knobs (pdcx/config.hpp:34-60 names where one exists):
+ *   "discarding_threshold" (double, default 0.7),
+ *   "recursion_dc"         (X used below level 0; 0 = same as level 0; default 3),
+ *   "small_threshold"      (texts up to this length are solved by the in-CTA
+ *                           base case; default 2048, max 2048),
+ *   "prefix_chars"         (chars in the first radix sort; 0 = auto),
+ *   "trace"                (1 = keep level-0 names/unique flags for dcx_get_trace). */
+int dcx_set_option(dcx_ctx* ctx, const char* name, double value);
+
+/* ---- single text ----------------------------------------------------------- */
+/* PDCX::compute_sa for one text of n bytes.  `dc` is X in {3,7,13,21,31,39,57,73,
+ * 91,95,133}.  Unless DCX_NO_REMAP, bytes are remapped to 1..sigma first (the
+ * reference cli's compress_alphabet).  A text that uses all 256 byte values is
+ * accepted and built with 257-symbol keys (the reference refuses it);
+ * dcx_build_sa_strict reproduces the refusal.  sa_out receives n entries of
+ * sa_width bits.  n must be < 2^32 - 1. */
+int dcx_build_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
+                 void* sa_out, uint32_t flags);
+/* Same as dcx_build_sa but refuses a 256-symbol alphabet (cli.cpp:440-446). */
+int dcx_build_sa_strict(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
+                        void* sa_out, uint32_t flags);
+
+/* Statistics of the last build on this context. */
+int dcx_get_stats(dcx_ctx* ctx, dcx_stats* out);
+
+/* Level-0 observations of the last build with option "trace" = 1: names and
+ * unique flags of the m level-0 samples in sample text order
+ * (slot = (i/X)*D + NEXT_RANK[i%X], pdcx/merge_samples.hpp:181-188). */
+int dcx_get_trace(dcx_ctx* ctx, uint64_t* m_out, uint32_t* names, uint8_t* unique, uint64_t capacity);
+
+/* ---- batch ----------------------------------------------------------------- */
+/* Builds one SA per text.  texts is the concatenation, offsets[num_texts+1] the
+ * text boundaries (offsets[0] = 0).  sa_out receives, per text, its SA with
+ * text-local indices, concatenated in the same layout as texts.  dc_or_auto = 0
+ * lets the autotuner pick X per size class.  Every text must be < 2^32 - 1 bytes;
+ * the concatenation may be larger than one build fits: it is split into rounds. */
+int dcx_build_sa_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offsets,
+                       uint32_t num_texts, int dc_or_auto, int sa_width, void* sa_out,
+                       uint32_t flags);
+
+/* ---- serving (continuous batching) ----------------------------------------- */
+/* Admits an SA request.  The text is copied at submission; the request is
+ * admitted to the GPU when its projected footprint fits the budget.  Returns
+ * DCX_ERR_BUDGET if the request can never fit. */
+int dcx_serve_submit(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
+                     uint64_t* req_id);
+/* Polls a request: *status = 0 queued, 1 running, 2 done, <0 failed (error code).
+ * When done and sa_host is non-null, copies the SA (n entries of sa_width bits)
+ * into sa_host.  latency_ms (optional) receives submit->done wall time. */
+int dcx_serve_poll(dcx_ctx* ctx, uint64_t req_id, void* sa_host, int* status, double* latency_ms);
+/* Frees a finished request's result. */
+int dcx_serve_release(dcx_ctx* ctx, uint64_t req_id);
+/* Blocks until every submitted request is done. */
+int dcx_serve_drain(dcx_ctx* ctx);
+
+/* ---- misc ------------------------------------------------------------------ */
+const char* dcx_strerror(int code);
+/* Difference-cover tables generated in closed form (pdcx/difference_cover.hpp):
+ * fills D, DC[D], NEXT_RANK[X] and cmpDepthRanks[X][X][3]; returns DCX_ERR_ARG
+ * for an unsupported X.  Host-only, needs no GPU. */
+int dcx_dc_table(int X, uint32_t* D, uint32_t* dc, uint32_t* next_rank, uint32_t* cmp_depth_ranks);
+/* Library version string. */
+const char* dcx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DCX_GPU_H */

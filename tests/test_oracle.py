@@ -1,0 +1,107 @@
+"""The CPU oracle (restatement of PDCX) pinned against the reference's own golden
+vectors and tables, and against libsais built from the reference tree."""
+import re
+
+import numpy as np
+import pytest
+
+from conftest import random_text, reference_file
+
+
+def test_golden_abracadabra(oracle):
+    for name in ("abracadabra4", "abracadabra8"):
+        text = np.fromfile(reference_file("B_DC_3_7_13", "src", "examples", name), np.uint8)
+        gold = np.fromfile(reference_file("B_DC_3_7_13", "src", "examples", name + ".sa"), np.uint32)
+        for X in (3, 7, 13, 39):
+            sa = oracle.dcx_sa(text, X=X, base_case_threshold=0)
+            assert np.array_equal(sa, gold.astype(np.uint64)), (name, X)
+        assert np.array_equal(oracle.libsais(text), gold.astype(np.int64))
+
+
+def test_golden_three_brothers(oracle):
+    text = np.fromfile(reference_file("dPD", "tests", "test_data", "the_three_brothers.txt"), np.uint8)
+    gold = np.fromfile(reference_file("dPD", "tests", "test_data", "the_three_brothers_size_t_sa"), np.uint64)
+    assert np.array_equal(oracle.libsais(text).astype(np.uint64), gold)
+    for X in (3, 7, 13, 39):
+        for packing in (True, False):
+            assert np.array_equal(oracle.dcx_sa(text, X=X, packing=packing, base_case_threshold=0), gold)
+
+
+def test_text_only_edge_files(oracle):
+    for rel in (("B_DC_3_7_13", "src", "examples", "aaa"), ("B_DC_3_7_13", "src", "examples", "mississippi"),
+                ("dPD", "tests", "test_data", "small_text.txt")):
+        text = np.fromfile(reference_file(*rel), np.uint8)
+        ref = oracle.libsais(text).astype(np.uint64)
+        for X in (3, 39):
+            assert np.array_equal(oracle.dcx_sa(text, X=X, base_case_threshold=0), ref)
+
+
+def _parse_reference_tables():
+    src = open(reference_file("lightweight_dcx", "src", "pdcx", "difference_cover.hpp")).read()
+    out = {}
+    for m in re.finditer(r"struct DC(\d+)Param \{(.*?)\n\};", src, re.S):
+        X = int(m.group(1))
+        body = m.group(2)
+        nums = lambda key: [int(v) for v in re.findall(r"\d+", re.search(key + r".*?=\s*(\{.*?\});", body, re.S).group(1))]
+        out[X] = (nums(r"DC\[D\]"), nums(r"NEXT_RANK\[X\]"), nums(r"cmpDepthRanks\[X\]\[X\]\[3\]"))
+    return out
+
+
+def test_dc_tables_closed_form_equal_reference(oracle):
+    ref = _parse_reference_tables()
+    assert set(ref) == {3, 7, 13, 21, 31, 39, 57, 73, 91, 95, 133}
+    for X, (dc, nr, cmp) in ref.items():
+        odc, _, onr, ocmp = oracle.dc_table(X)
+        assert list(odc) == dc
+        assert list(onr) == nr
+        assert list(ocmp.ravel()) == cmp, X
+
+
+@pytest.mark.parametrize("X", [3, 7, 13, 39])
+def test_difference_cover_property(oracle, X):
+    dc, in_dc, _, _ = oracle.dc_table(X)
+    diffs = {(int(a) - int(b)) % X for a in dc for b in dc}
+    assert diffs == set(range(X))
+
+
+@pytest.mark.parametrize("X", [3, 7, 13, 39])
+def test_reference_test_matrix(oracle, X):
+    """main.cpp:80-123 matrix (sigma in {2,8,32}) with a small base case so the DCX
+    phases run, plus the alignment sweep n = 1000 + d."""
+    for sigma in (2, 8, 32):
+        for n, reps in ((100, 6), (1000, 3), (10000, 1)):
+            for r in range(reps):
+                t = random_text(n, sigma, seed=r * 7 + sigma)
+                assert np.array_equal(oracle.dcx_sa(t, X=X, base_case_threshold=0),
+                                      oracle.libsais(t).astype(np.uint64))
+        for d in range(15):
+            t = random_text(1000 + d, sigma, seed=d)
+            assert np.array_equal(oracle.dcx_sa(t, X=X, base_case_threshold=0),
+                                  oracle.libsais(t).astype(np.uint64))
+
+
+def test_recursion_and_discarding_paths(oracle):
+    t = np.tile(np.frombuffer(b"ACGTTGCAAC", np.uint8), 600)
+    sa, tr = oracle.dcx_sa(t, X=39, base_case_threshold=0, want_trace=True)
+    assert tr.recursion in (1, 2) and tr.max_depth > 1
+    assert np.array_equal(sa, oracle.libsais(t).astype(np.uint64))
+    rng = np.random.default_rng(3)
+    base = rng.integers(0, 4, 3000).astype(np.uint8) + 65
+    t2 = np.concatenate([base, base[:2000], rng.integers(65, 69, 3000).astype(np.uint8)])
+    sa2, tr2 = oracle.dcx_sa(t2, X=7, base_case_threshold=0, want_trace=True)
+    assert tr2.recursion == 2 and tr2.reduction <= 0.7
+    assert np.array_equal(sa2, oracle.libsais(t2).astype(np.uint64))
+
+
+def test_alphabet_256_refused(oracle):
+    t = np.arange(512, dtype=np.uint32).astype(np.uint8)
+    with pytest.raises(ValueError):
+        oracle.compress_alphabet(t)
+
+
+def test_packing_choice(oracle):
+    # cli.cpp:488-533: 3/5/8 bits, K = ceil(X / (64 / bits))
+    assert oracle.packing_for_sigma(39, 4) == (3, 2)
+    assert oracle.packing_for_sigma(3, 4) == (3, 1)
+    assert oracle.packing_for_sigma(39, 20) == (5, 4)
+    assert oracle.packing_for_sigma(39, 200) == (8, 5)
