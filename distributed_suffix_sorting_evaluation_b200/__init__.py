@@ -46,7 +46,7 @@ SUPPORTED_DC = (3, 7, 13, 21, 31, 39, 57, 73, 91, 95, 133)
 # Every exported symbol of include/dcx_gpu.h (checked by the CPU test suite).
 EXPORTED = (
     "dcx_ctx_create", "dcx_ctx_destroy", "dcx_set_option", "dcx_build_sa", "dcx_build_sa_strict",
-    "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
+    "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
 )
 
@@ -93,6 +93,7 @@ def load_library(path: str | None = None):
     lib.dcx_build_sa.argtypes = [vp, vp, u64, i32, i32, vp, u32]
     lib.dcx_build_sa_strict.argtypes = [vp, vp, u64, i32, i32, vp, u32]
     lib.dcx_get_stats.argtypes = [vp, ctypes.POINTER(DcxStats)]
+    lib.dcx_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.dcx_get_trace.argtypes = [vp, ctypes.POINTER(u64), vp, vp, u64]
     lib.dcx_build_sa_batch.argtypes = [vp, vp, vp, u32, i32, i32, vp, u32]
     lib.dcx_serve_submit.argtypes = [vp, vp, u64, i32, i32, ctypes.POINTER(u64)]
@@ -187,6 +188,19 @@ class Context:
                         packing: bool = True):
         """SA of a device-resident text into a device buffer (both raw CUDA pointers)."""
         flags = DCX_DEVICE_PTRS | (0 if packing else DCX_NO_PACKING)
+        _check(self.lib.dcx_build_sa(self.h, ctypes.c_void_p(text_ptr), n, dc, sa_width, ctypes.c_void_p(sa_ptr),
+                                     flags))
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""
+        p = ctypes.c_void_p()
+        _check(self.lib.dcx_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def build_sa_hostptr(self, text_ptr: int, n: int, sa_ptr: int, dc: int = 39, sa_width: int = 40,
+                         packing: bool = True):
+        """SA of a text in (pinned) host memory into host memory: the end-to-end call."""
+        flags = DCX_HOST_PTRS | (0 if packing else DCX_NO_PACKING)
         _check(self.lib.dcx_build_sa(self.h, ctypes.c_void_p(text_ptr), n, dc, sa_width, ctypes.c_void_p(sa_ptr),
                                      flags))
 

@@ -2,6 +2,7 @@
 
   lib/libdcxgpu.so  -- the CUDA engine and its C ABI (include/dcx_gpu.h)
   lib/dcx_cli       -- the reference-compatible command line front end
+  lib/libtextgen.so -- seeded synthetic text generators of the benchmark workloads
 
 Run as ``python -m distributed_suffix_sorting_evaluation_b200.build``.
 nvcc cross-compiles, so no GPU is needed to build.
@@ -55,6 +56,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
         cuda_lib = "/usr/local/cuda/lib64"
         cmd = [HOST_CXX, "-O2", "-std=c++17", f"-I{INC}", "-o", cli, cli_src, f"-L{LIB}", "-ldcxgpu",
                f"-L{cuda_lib}", "-lcudart", "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{cuda_lib}", "-lpthread"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    gen = os.path.join(LIB, "libtextgen.so")
+    gen_src = os.path.join(CSRC, "textgen.cpp")
+    if force or _stale(gen, [gen_src]):
+        cmd = [HOST_CXX, "-O2", "-std=c++17", "-fopenmp", "-shared", "-fPIC", "-o", gen, gen_src]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -107,14 +107,17 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
+// Loads are warp-striped: lane l of warp w reads element w*32*ITEMS + it*32 + l
+// of the tile in iteration it, so every load instruction is coalesced.
 template <typename T, typename Op>
 __global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(Op op, uint64_t n, T* tile_sums) {
     __shared__ T sm[SCAN_THREADS / 32 + 1];
-    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)(threadIdx.x >> 5) * 32 * SCAN_ITEMS +
+                          (threadIdx.x & 31);
     T acc = T(0);
 #pragma unroll
     for (int it = 0; it < SCAN_ITEMS; it++) {
-        uint64_t i = base + (uint64_t)it * SCAN_THREADS + threadIdx.x;
+        const uint64_t i = base + (uint64_t)it * 32;
         if (i < n) acc += op.load(i);
     }
     T total;
@@ -138,25 +141,26 @@ __global__ __launch_bounds__(1024) void k_scan_tile_sums(T* sums, uint64_t count
     if (threadIdx.x == 0 && grand_total) *grand_total = carry;
 }
 
+// Apply phase: thread t owns SCAN_ITEMS consecutive elements of the tile (each
+// thread's loads walk one contiguous 16-element run, fully used through L1).
 template <typename T, typename Op>
 __global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(Op op, uint64_t n, const T* tile_prefix) {
     __shared__ T sm[SCAN_THREADS / 32 + 1];
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
     T vals[SCAN_ITEMS];
     T acc = T(0);
-    // blocked layout: thread t owns items [t*ITEMS, (t+1)*ITEMS) of the tile
 #pragma unroll
     for (int it = 0; it < SCAN_ITEMS; it++) {
-        uint64_t i = base + it;
+        const uint64_t i = base + it;
         vals[it] = i < n ? op.load(i) : T(0);
         acc += vals[it];
     }
     T total;
-    T ex = block_excl_scan<SCAN_THREADS>(acc, sm, total);
+    const T ex = block_excl_scan<SCAN_THREADS>(acc, sm, total);
     T run = tile_prefix[blockIdx.x] + ex;
 #pragma unroll
     for (int it = 0; it < SCAN_ITEMS; it++) {
-        uint64_t i = base + it;
+        const uint64_t i = base + it;
         if (i < n) op.store(i, run, vals[it]);
         run += vals[it];
     }

@@ -133,19 +133,21 @@ static uint32_t key_bits(uint64_t B, uint32_t P) {
     return std::max<uint32_t>(1, x.bits_of_minus_one());
 }
 
-static uint32_t max_chars_in(uint64_t B, uint32_t words) {
+static uint32_t max_chars_in_bits(uint64_t B, uint32_t bits) {
     uint32_t P = 0;
     BigUInt x;
     while (true) {
         BigUInt y = x;
         y.mul((uint32_t)B);
-        if (y.bits_of_minus_one() > 32 * words) break;
+        if (y.bits_of_minus_one() > bits) break;
         x = y;
         P++;
         if (P > 4096) break;
     }
     return P;
 }
+
+static uint32_t max_chars_in(uint64_t B, uint32_t words) { return max_chars_in_bits(B, 32 * words); }
 
 static KeyPlan make_plan(uint64_t B, uint32_t P) {
     KeyPlan p{};
@@ -226,6 +228,7 @@ struct Ctx {
     std::map<uint32_t, DcFlags*> dc_flags_dev;  // per X (samples_before filled per level on a copy)
     std::map<uint32_t, DcDev*> dc_dev;
     // trace of level 0
+    double level0_entropy = 0;  // order-0 entropy (bits/char) of the current level-0 text
     std::vector<uint32_t> trace_names;
     std::vector<uint8_t> trace_uniq;
     std::mutex build_mu;
@@ -366,7 +369,7 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         }
     }
     if (run.empty()) return 0;
-    constexpr int ITEMS = 16;
+    constexpr int ITEMS = 12;  // 64 registers: 4 CTAs per SM (measured best on B200)
     constexpr int TILE = SORT_THREADS * ITEMS;
     const uint64_t tiles = div_up(count, TILE);
     if (tiles > c.lookback_tiles) {
@@ -406,7 +409,7 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         a.epoch = c.epoch;
         a.err = c.d_err;
         a.spin_limit = c.opt.spin_limit;
-        k_onesweep<ITEMS><<<(unsigned)tiles, SORT_THREADS, 0, c.stream>>>(a);
+        k_onesweep_ec<ITEMS, true><<<(unsigned)tiles, SORT_THREADS, 0, c.stream>>>(a);
         DCX_CHECK_LAUNCH();
         cur ^= 1;
     }
@@ -438,6 +441,18 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
     const uint32_t words_full = (key_bits(B, L) + 31) / 32;
     uint32_t kw0_max = depth == 0 ? 2 : 3;
     uint32_t P0 = std::min<uint32_t>(L, max_chars_in(B, std::min(words_full, kw0_max)));
+    if (depth == 0 && c.level0_entropy > 0.05) {
+        // Shortest byte-aligned prefix whose expected random collisions stay near
+        // 1% of N: P * H >= log2(N) + 7, with H the order-0 entropy discounted by
+        // 15% for context dependence.  Ties left over are resolved exactly by the
+        // refinement rounds, so this only trades passes against refinement work.
+        const double need = std::log2((double)N) + 7.0;
+        uint32_t P = (uint32_t)std::ceil(need / (0.85 * c.level0_entropy));
+        P = std::max<uint32_t>(1, std::min(P, P0));
+        const uint32_t bytes = (key_bits(B, P) + 7) / 8;
+        const uint32_t fill = std::min<uint32_t>(P0, max_chars_in_bits(B, 8 * bytes));
+        P0 = std::max(P, fill);
+    }
     if (c.opt.prefix_chars && depth == 0) P0 = std::min<uint32_t>(L, c.opt.prefix_chars);
     if (P0 == 0) P0 = 1;
     KeyPlan plan = make_plan(B, P0);
@@ -461,8 +476,20 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
         KeyOut ko{};
         for (uint32_t w = 0; w < kw; w++) ko.w[w] = s.k[0][w];
         const int grid = grid_for(N, 256, 148 * 8);
-        const size_t shm = 4 * kw * RADIX * 4;
-        if (kw == 1) k_keys_prefix<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
+        const size_t shm = (size_t)HIST_COPIES * 4 * kw * RADIX * 4;
+        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<1, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<2, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<3, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+        if (kw <= 2 && P0 <= (uint32_t)SLIDE_MAX_CHARS) {
+            // sliding-window builder: keys of consecutive positions share P-1 chars
+            uint64_t pow_top = 1;
+            for (uint32_t i = 1; i < P0; i++) pow_top *= B;
+            const size_t sshm = keys_slide_smem<CharT>();
+            DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
+            const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 3);
+            k_keys_slide<CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, n, N, plan, pow_top, ko, s.v[0],
+                                                                         c.d_hist);
+        } else if (kw == 1) k_keys_prefix<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
         else if (kw == 2) k_keys_prefix<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
         else k_keys_prefix<3, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
         DCX_CHECK_LAUNCH();
@@ -482,8 +509,8 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
     // refinement rounds for tied windows
     uint32_t covered = P0;
     while (covered < L) {
-        DBuf<uint32_t> slot(&c, N), grp(&c, N);
-        OpTied op{head.get(), N, slot.get(), grp.get()};
+        DBuf<uint32_t> slot(&c, N), grp(&c, N), tpos(&c, N);
+        OpTied op{head.get(), N, sa.get(), slot.get(), grp.get(), tpos.get()};
         const uint64_t tot = device_scan<uint64_t>(c, op, N);
         c.alg(N + N / 2);
         const uint64_t cnt = tot >> 32;
@@ -506,13 +533,15 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
         KeyOut ko{};
         for (uint32_t w = 0; w < kwr; w++) ko.w[w] = s.k[0][w];
         const int grid = grid_for(cnt, 256, 148 * 8);
-        const size_t shm = 4 * kwr * RADIX * 4;
+        const size_t shm = (size_t)HIST_COPIES * 4 * kwr * RADIX * 4;
+        DCX_CUDA(cudaFuncSetAttribute(k_keys_refine<1, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+        DCX_CUDA(cudaFuncSetAttribute(k_keys_refine<2, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
         if (rp.kw == 1)
-            k_keys_refine<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, slot.get(), grp.get(), sa.get(),
-                                                                  covered, rp, ko, s.v[0], c.d_hist);
+            k_keys_refine<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, tpos.get(), grp.get(), covered, rp,
+                                                                  ko, s.v[0], c.d_hist);
         else
-            k_keys_refine<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, slot.get(), grp.get(), sa.get(),
-                                                                  covered, rp, ko, s.v[0], c.d_hist);
+            k_keys_refine<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, tpos.get(), grp.get(), covered, rp,
+                                                                  ko, s.v[0], c.d_hist);
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(cnt * (12 + Pr * sizeof(CharT)) + cnt * (kwr + 1) * 4);
@@ -672,7 +701,7 @@ struct LevelInfo {
 
 template <typename CharT>
 static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_t X, int depth, bool packing,
-                  uint32_t* sa_out);
+                  void* sa_out, int out_width = 32);
 
 static void small_sa_single(Ctx& c, const void* text, bool wide, uint64_t n, uint32_t* sa_out) {
     uint64_t offs[2] = {0, n};
@@ -700,12 +729,21 @@ static uint32_t level0_sample_chars(uint32_t X, uint64_t sigma, bool packing) {
 
 template <typename CharT>
 static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_t X, int depth, bool packing,
-                  uint32_t* sa_out) {
+                  void* sa_out, int out_width) {
     if (n == 0) return;
     if (depth > 64) throw Error(DCX_ERR_INTERNAL, "recursion deeper than 64 levels");
     c.st.levels = std::max<uint32_t>(c.st.levels, (uint32_t)depth + 1);
     if (n <= c.opt.small_threshold && n <= (uint64_t)SMALL_MAX) {
-        small_sa_single(c, text, sizeof(CharT) == 4, n, sa_out);
+        if (out_width == 32) {
+            small_sa_single(c, text, sizeof(CharT) == 4, n, (uint32_t*)sa_out);
+        } else {
+            DBuf<uint32_t> tmp(&c, n);
+            small_sa_single(c, text, sizeof(CharT) == 4, n, tmp.get());
+            k_widen<<<grid_for(n, 256), 256, 0, c.stream>>>(tmp.get(), n, (uint8_t*)sa_out, out_width);
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            DCX_CUDA(cudaStreamSynchronize(c.stream));
+        }
         return;
     }
     const DcHost& dc = get_dc(c, X);
@@ -746,6 +784,7 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
     sort_windows<CharT>(c, text, n, B, L, depth, sa, head);
 
     // ---- phase 2: names
+    if (m >= (1ull << 31)) throw Error(DCX_ERR_ARG, "more than 2^31 samples in one level");
     DBuf<uint32_t> s_pos(&c, m), s_grp(&c, m);
     {
         OpSamples op{head.get(), sa.get(), dfl.get(), s_pos.get(), s_grp.get(), m};
@@ -762,6 +801,15 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
     }
     s_grp.reset();
     const uint32_t last_rank = d2h_scalar(c, name.get() + (m - 1));
+    // sample records in sample text order (one random scatter)
+    DBuf<uint64_t> srec(&c, m);
+    k_scatter_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), uniq.get(), dfl.get(),
+                                                             srec.get());
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    c.alg(m * 17);
+    s_pos.reset();
+    uniq.reset();
     if (depth == 0) {
         c.st.level0_samples = m;
         c.st.level0_last_rank = last_rank;
@@ -770,8 +818,7 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
         if (c.opt.trace) {
             DBuf<uint32_t> tn(&c, m);
             DBuf<uint8_t> tu(&c, m);
-            k_scatter_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), dfl.get(), nullptr,
-                                                                   tn.get(), tu.get(), uniq.get());
+            k_ranks_from_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), nullptr, tn.get(), tu.get());
             DCX_CHECK_LAUNCH();
             c.trace_names.resize(m);
             c.trace_uniq.resize(m);
@@ -782,24 +829,23 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
     }
     cudaEventRecord(ev[1], c.stream);
 
-    // ---- phase 3: ranks of the samples (sample text order, D zero slots of padding)
+    // ---- phase 3: ranks of the samples in sample text order, D zero slots of padding
     DBuf<uint32_t> rank_text(&c, m + D);
-    DCX_CUDA(cudaMemsetAsync(rank_text.get(), 0, (m + D) * 4, c.stream));
+    DCX_CUDA(cudaMemsetAsync(rank_text.get() + m, 0, D * 4, c.stream));
     if (last_rank >= m) {
-        k_scatter_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), dfl.get(), rank_text.get(),
-                                                               nullptr, nullptr, nullptr);
+        name.reset();
+        k_ranks_from_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), rank_text.get(), nullptr, nullptr);
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(m * 12);
     } else {
         const uint32_t Xr = c.opt.recursion_dc ? c.opt.recursion_dc : X;
-        DBuf<uint32_t> rec(&c, m), q_of_j(&c, m);
+        DBuf<uint32_t> rec(&c, m);
         DBuf<uint8_t> rec_uniq(&c, m);
-        k_build_rec<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), uniq.get(), dfl.get(),
-                                                           rec.get(), rec_uniq.get(), q_of_j.get());
+        k_rec_from_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), dfl.get(), rec.get(), rec_uniq.get());
         DCX_CHECK_LAUNCH();
         c.launched();
-        c.alg(m * 21);
+        c.alg(m * 13);
         // discarding decision (pdcx.hpp:150-165)
         DBuf<uint32_t> kidx(&c, m);
         OpKeep kop{rec_uniq.get(), rec.get(), nullptr, kidx.get()};
@@ -813,8 +859,9 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
         }
         if (!discard) {
             kidx.reset();
-            q_of_j.reset();
             rec_uniq.reset();
+            srec.reset();
+            name.reset();
             DBuf<uint32_t> sa_r(&c, m);
             level<uint32_t>(c, rec.get(), m, last_rank, Xr, depth + 1, false, sa_r.get());
             rec.reset();
@@ -837,26 +884,33 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
             DCX_CHECK_LAUNCH();
             c.launched();
             sa2.reset();
-            // non-unique samples keyed by (name, rank2)
+            // unique samples keep their window order
+            k_ranks_unique_text<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), rank_text.get());
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            c.alg(m * 12);
+            // non-unique samples keyed by (name, rank2) (pdcx.hpp:296-346)
+            const uint64_t mu_cap = m - 0;  // upper bound
             DBuf<uint32_t> keys[2][2];
             DBuf<uint32_t> vals[2];
             SortSpace s;
-            for (int b = 0; b < 2; b++) {
-                for (int w = 0; w < 2; w++) {
-                    keys[b][w] = DBuf<uint32_t>(&c, m);
-                    s.k[b][w] = keys[b][w].get();
-                }
-                vals[b] = DBuf<uint32_t>(&c, m);
-                s.v[b] = vals[b].get();
-            }
-            OpNonUnique nop{uniq.get(), name.get(), q_of_j.get(), kidx.get(), rank_of.get(), s.k[0][0], s.k[0][1],
-                            s.v[0]};
-            const uint32_t mu = device_scan<uint32_t>(c, nop, m);
-            c.alg(m + mu * 24);
-            rank_of.reset();
-            kidx.reset();
-            q_of_j.reset();
+            const uint32_t mu = device_scan<uint32_t>(
+                c, OpNonUniqueText{srec.get(), dfl.get(), kidx.get(), rank_of.get(), nullptr, nullptr, nullptr}, m);
+            (void)mu_cap;
             if (mu) {
+                for (int bb = 0; bb < 2; bb++) {
+                    for (int w = 0; w < 2; w++) {
+                        keys[bb][w] = DBuf<uint32_t>(&c, mu);
+                        s.k[bb][w] = keys[bb][w].get();
+                    }
+                    vals[bb] = DBuf<uint32_t>(&c, mu);
+                    s.v[bb] = vals[bb].get();
+                }
+                OpNonUniqueText nop{srec.get(), dfl.get(), kidx.get(), rank_of.get(), s.k[0][0], s.k[0][1], s.v[0]};
+                device_scan<uint32_t>(c, nop, m);
+                c.alg(m * 9 + mu * 24);
+                rank_of.reset();
+                kidx.reset();
                 DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
                 SortPassArgs ha{};
                 ha.keys_in[0] = s.k[0][0];
@@ -871,32 +925,26 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
                 DBuf<uint32_t> start_s(&c, (uint64_t)last_rank + 1), start_l(&c, (uint64_t)last_rank + 1);
                 k_name_starts<<<grid_for(m, 256), 256, 0, c.stream>>>(m, name.get(), start_s.get());
                 k_name_starts<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], start_l.get());
-                k_ranks_after_discarding<<<grid_for(mu, 256), 256, 0, c.stream>>>(
-                    mu, s.k[f][1], s.v[f], start_s.get(), start_l.get(), s_pos.get(), dfl.get(), rank_text.get());
+                k_ranks_nonunique<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], s.v[f], start_s.get(),
+                                                                          start_l.get(), rank_text.get());
                 DCX_CHECK_LAUNCH();
                 c.launched(3);
                 c.alg(m * 8 + mu * 8 + mu * 24);
             }
-            k_ranks_unique<<<grid_for(m, 256), 256, 0, c.stream>>>(m, uniq.get(), s_pos.get(), dfl.get(),
-                                                                  rank_text.get());
-            DCX_CHECK_LAUNCH();
-            c.launched();
-            c.alg(m * 9);
         }
     }
-    s_pos.reset();
+    srec.reset();
     name.reset();
-    uniq.reset();
     cudaEventRecord(ev[2], c.stream);
 
     // ---- phase 4: tie groups, then emit
     tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc);
     head.reset();
     rank_text.reset();
-    k_emit32<<<grid_for(n, 256), 256, 0, c.stream>>>(sa.get(), n, sa_out);
+    k_emit<<<grid_for(n / 4 + 1, 256), 256, 0, c.stream>>>(sa.get(), n, sa_out, out_width);
     DCX_CHECK_LAUNCH();
     c.launched();
-    c.alg(n * 8);
+    c.alg(n * (4 + out_width / 8));
     cudaEventRecord(ev[3], c.stream);
     DCX_CUDA(cudaEventSynchronize(ev[3]));
     if (depth == 0) {
@@ -957,6 +1005,12 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         DCX_CUDA(cudaMemcpyAsync(h, c.d_h256, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
         DCX_CUDA(cudaStreamSynchronize(c.stream));
         if (h[0]) throw Error(DCX_ERR_ARG, "char 0 is reserved for padding");
+        c.level0_entropy = 0;
+        for (int i = 1; i < 256; i++)
+            if (h[i]) {
+                const double p = (double)h[i] / (double)n;
+                c.level0_entropy -= p * std::log2(p);
+            }
         for (int i = 255; i > 0; i--)
             if (h[i]) {
                 sigma = i;
@@ -971,8 +1025,13 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         DCX_CUDA(cudaStreamSynchronize(c.stream));
         ByteMap map{};
         uint32_t next = 1;
+        c.level0_entropy = 0;
         for (int i = 0; i < 256; i++)
-            if (h[i]) map.m[i] = (uint8_t)(next++);
+            if (h[i]) {
+                map.m[i] = (uint8_t)(next++);
+                const double p = (double)h[i] / (double)n;
+                c.level0_entropy -= p * std::log2(p);
+            }
         sigma = next - 1;
         if (sigma == 256 && strict)
             throw Error(DCX_ERR_ALPHABET, "256 distinct symbols: 0 is reserved for padding");
@@ -984,13 +1043,13 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     c.alg(n * 3);
     c.st.sigma = (uint32_t)sigma;
     cudaEventRecord(e2, c.stream);
-    DBuf<uint32_t> sa32;
-    uint32_t* out32 = nullptr;
-    if (dev && width == 32) {
-        out32 = (uint32_t*)sa_out;
-    } else {
-        sa32 = DBuf<uint32_t>(&c, n);
-        out32 = sa32.get();
+    // SA straight into the caller's device buffer, or into a staging buffer for host pointers
+    const size_t wb = width / 8;
+    DBuf<uint8_t> stage;
+    void* dout = sa_out;
+    if (!dev || ((uintptr_t)sa_out & 15)) {
+        stage = DBuf<uint8_t>(&c, n * wb + 16);
+        dout = stage.get();
     }
     if (wide_text) {
         // all 256 byte values occur: remap b -> b + 1 into 32-bit chars and build
@@ -1001,30 +1060,24 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         c.launched();
         t_in.reset();
         t_map.reset();
-        level<uint32_t>(c, t32.get(), n, sigma, (uint32_t)X, 0, packing, out32);
+        level<uint32_t>(c, t32.get(), n, sigma, (uint32_t)X, 0, packing, dout, width);
     } else {
         t_in.reset();
-        level<uint8_t>(c, t_map.get(), n, sigma, (uint32_t)X, 0, packing, out32);
+        level<uint8_t>(c, t_map.get(), n, sigma, (uint32_t)X, 0, packing, dout, width);
     }
     t_map.reset();
-    DBuf<uint8_t> wide;
-    if (width != 32) {
-        uint8_t* wout = dev ? (uint8_t*)sa_out : nullptr;
-        if (!dev) {
-            wide = DBuf<uint8_t>(&c, n * (width / 8));
-            wout = wide.get();
-        }
-        k_widen<<<grid_for(n, 256), 256, 0, c.stream>>>(out32, n, wout, width);
-        DCX_CHECK_LAUNCH();
-        c.launched();
-        c.alg(n * (4 + width / 8));
-    }
+    if (dev && dout != sa_out)
+        DCX_CUDA(cudaMemcpyAsync(sa_out, dout, n * wb, cudaMemcpyDeviceToDevice, c.stream));
     cudaEventRecord(e3, c.stream);
-    if (!dev) {
-        const void* src = width == 32 ? (const void*)out32 : (const void*)wide.get();
-        DCX_CUDA(cudaMemcpyAsync(sa_out, src, n * (width / 8), cudaMemcpyDeviceToHost, c.stream));
-    }
+    cudaEvent_t e4;
+    cudaEventCreate(&e4);
+    if (!dev) DCX_CUDA(cudaMemcpyAsync(sa_out, dout, n * wb, cudaMemcpyDeviceToHost, c.stream));
+    cudaEventRecord(e4, c.stream);
     DCX_CUDA(cudaStreamSynchronize(c.stream));
+    float d2h = 0;
+    cudaEventElapsedTime(&d2h, e3, e4);
+    c.st.ms_d2h = d2h;
+    cudaEventDestroy(e4);
     float h2d = 0, p0 = 0, total = 0;
     cudaEventElapsedTime(&h2d, e0, e1);
     cudaEventElapsedTime(&p0, e1, e2);
@@ -1179,6 +1232,12 @@ int dcx_build_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, voi
 
 int dcx_build_sa_strict(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags) {
     return build_entry(x, text, n, dc, w, out, flags, true);
+}
+
+int dcx_get_stream(dcx_ctx* x, void** out) {
+    if (!x || !out) return DCX_ERR_ARG;
+    *out = (void*)x->c.stream;
+    return DCX_OK;
 }
 
 int dcx_get_stats(dcx_ctx* x, dcx_stats* out) {

@@ -67,12 +67,33 @@ struct KeyOut {
     uint32_t* w[MAX_KEY_WORDS];
 };
 
+// Adds one key's 8-bit digits of all 4*KW passes to the block histograms
+// (static word/byte indexing keeps the key in registers).
+// Each pair of warps owns a private copy of the histograms (HIST_COPIES copies
+// per block), so near-constant top digits contend only within two warps.
+constexpr int HIST_COPIES = 4;
+
 template <int KW>
-__device__ __forceinline__ void hist_add(uint32_t* sh, const uint32_t* key, uint32_t passes) {
-    for (uint32_t p = 0; p < passes; p++) {
-        uint32_t s = p * RADIX_BITS;
-        uint32_t d = (key[s >> 5] >> (s & 31)) & (RADIX - 1);
-        atomicAdd(&sh[p * RADIX + d], 1u);
+__device__ __forceinline__ void hist_add(uint32_t* sh, const uint32_t* key) {
+    uint32_t* h = sh + (threadIdx.x >> 6) * (4 * KW * RADIX);
+#pragma unroll
+    for (int w = 0; w < KW; w++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) atomicAdd(&h[(4 * w + b) * RADIX + ((key[w] >> (8 * b)) & (RADIX - 1))], 1u);
+}
+
+// Zero the private copies / fold them into the global histogram.
+__device__ __forceinline__ void hist_zero(uint32_t* sh, uint32_t bins) {
+    for (uint32_t i = threadIdx.x; i < HIST_COPIES * bins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+}
+__device__ __forceinline__ void hist_flush(const uint32_t* sh, uint32_t bins, uint32_t* hist) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int c = 0; c < HIST_COPIES; c++) v += sh[c * bins + i];
+        if (v) atomicAdd(&hist[i], v);
     }
 }
 
@@ -82,52 +103,102 @@ template <int KW, typename CharT>
 __global__ __launch_bounds__(256) void k_keys_prefix(const CharT* __restrict__ text, uint64_t n, uint64_t N,
                                                      KeyPlan plan, KeyOut ko, uint32_t* __restrict__ vals_out,
                                                      uint32_t* hist) {
-    extern __shared__ uint32_t sh[];
-    const uint32_t total_passes = 4 * KW;
-    for (uint32_t i = threadIdx.x; i < total_passes * RADIX; i += blockDim.x) sh[i] = 0;
-    __syncthreads();
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*KW * RADIX
+    hist_zero(sh, 4 * KW * RADIX);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t key[KW];
         encode_window<KW>(text, n, i, plan, key);
 #pragma unroll
         for (int w = 0; w < KW; w++) ko.w[w][i] = key[w];
         vals_out[i] = (uint32_t)i;
-        hist_add<KW>(sh, key, total_passes);
+        hist_add<KW>(sh, key);
     }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < total_passes * RADIX; i += blockDim.x)
-        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+    hist_flush(sh, 4 * KW * RADIX, hist);
 }
 
-// Refinement keys for the elements of tie groups: element j sits at sorted slot
-// slot[j]; its text position is sa[slot[j]], its group number grp[j].  The key is
+// Level keys for windows that fit 64 bits, built with a sliding window: a CTA
+// stages SLIDE_TILE + chars of text in shared memory, thread t encodes the
+// SLIDE_R consecutive positions [t*R, t*R + R) of the tile (one full encode,
+// then key' = (key - c_i * B^(P-1)) * B + c_{i+P} per step), and the keys are
+// written back through shared memory so global stores stay coalesced.  Chars
+// past the end of the text read as 0 (the padding char).
+constexpr int SLIDE_THREADS = 256;
+constexpr int SLIDE_R = 16;
+constexpr int SLIDE_TILE = SLIDE_THREADS * SLIDE_R;
+constexpr int SLIDE_MAX_CHARS = 64;
+
+template <typename CharT>
+__global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __restrict__ text, uint64_t n, uint64_t N,
+                                                              KeyPlan plan, uint64_t pow_top, KeyOut ko,
+                                                              uint32_t* __restrict__ vals_out, uint32_t* hist) {
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 8 * RADIX histogram words, then the staging area
+    uint32_t* hst = sh;
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 8 * RADIX);  // SLIDE_TILE keys
+    CharT* s_chars = reinterpret_cast<CharT*>(s_keys + SLIDE_TILE);             // SLIDE_TILE + P chars
+    hist_zero(hst, 8 * RADIX);
+    const uint32_t P = plan.chars;
+    const uint64_t B = plan.base;
+    for (uint64_t base = (uint64_t)blockIdx.x * SLIDE_TILE; base < N; base += (uint64_t)gridDim.x * SLIDE_TILE) {
+        for (uint32_t i = threadIdx.x; i < SLIDE_TILE + P; i += SLIDE_THREADS) {
+            const uint64_t p = base + i;
+            s_chars[i] = p < n ? text[p] : CharT(0);
+        }
+        __syncthreads();
+        const uint32_t r0 = threadIdx.x * SLIDE_R;
+        uint64_t key = 0;
+        for (uint32_t j = 0; j < P; j++) key = key * B + (uint32_t)s_chars[r0 + j];
+#pragma unroll
+        for (int r = 0; r < SLIDE_R; r++) {
+            s_keys[r0 + r] = key;
+            const uint32_t out = (uint32_t)s_chars[r0 + r];
+            key = (key - (uint64_t)out * pow_top) * B + (uint32_t)s_chars[r0 + r + P];
+        }
+        __syncthreads();
+        const uint32_t tile_n = (uint32_t)((N - base) < SLIDE_TILE ? (N - base) : SLIDE_TILE);
+        for (uint32_t i = threadIdx.x; i < tile_n; i += SLIDE_THREADS) {
+            const uint64_t k = s_keys[i];
+            uint32_t kk[2] = {(uint32_t)k, (uint32_t)(k >> 32)};
+            ko.w[0][base + i] = kk[0];
+            if (plan.kw > 1) ko.w[1][base + i] = kk[1];
+            vals_out[base + i] = (uint32_t)(base + i);
+            if (plan.kw > 1) hist_add<2>(hst, kk);
+            else hist_add<1>(hst, kk);
+        }
+        __syncthreads();
+    }
+    hist_flush(hst, 4 * plan.kw * RADIX, hist);
+}
+
+template <typename CharT>
+constexpr size_t keys_slide_smem() {
+    return sizeof(uint32_t) * HIST_COPIES * 8 * RADIX + sizeof(uint64_t) * SLIDE_TILE +
+           sizeof(CharT) * (SLIDE_TILE + SLIDE_MAX_CHARS);
+}
+
+// Refinement keys for the elements of tie groups: element j has text position
+// tpos[j] and group number grp[j].  The key is
 // (group number in the top word, window [pos+off, pos+off+chars) below it);
 // value = text position.
 template <int KW, typename CharT>
 __global__ __launch_bounds__(256) void k_keys_refine(const CharT* __restrict__ text, uint64_t n, uint64_t count,
-                                                     const uint32_t* __restrict__ slot,
-                                                     const uint32_t* __restrict__ grp,
-                                                     const uint32_t* __restrict__ sa, uint32_t off,
+                                                     const uint32_t* __restrict__ tpos,
+                                                     const uint32_t* __restrict__ grp, uint32_t off,
                                                      KeyPlan plan, KeyOut ko, uint32_t* __restrict__ vals_out,
                                                      uint32_t* hist) {
-    extern __shared__ uint32_t sh[];
-    const uint32_t total_passes = 4 * (KW + 1);
-    for (uint32_t i = threadIdx.x; i < total_passes * RADIX; i += blockDim.x) sh[i] = 0;
-    __syncthreads();
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*(KW+1) * RADIX
+    hist_zero(sh, 4 * (KW + 1) * RADIX);
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < count;
          j += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t pos = sa[slot[j]];
+        const uint32_t pos = tpos[j];
         uint32_t key[KW + 1];
         encode_window<KW>(text, n, (uint64_t)pos + off, plan, key);
         key[KW] = grp[j];
 #pragma unroll
         for (int w = 0; w <= KW; w++) ko.w[w][j] = key[w];
         vals_out[j] = pos;
-        hist_add<KW + 1>(sh, key, total_passes);
+        hist_add<KW + 1>(sh, key);
     }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < total_passes * RADIX; i += blockDim.x)
-        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+    hist_flush(sh, 4 * (KW + 1) * RADIX, hist);
 }
 
 }  // namespace dcx

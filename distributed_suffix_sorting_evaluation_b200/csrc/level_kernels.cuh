@@ -99,8 +99,10 @@ __global__ void k_heads(KeyWords k, uint32_t kw, uint64_t N, uint8_t* __restrict
 struct OpTied {
     const uint8_t* head;
     uint64_t N;
+    const uint32_t* sa;
     uint32_t* slot;
     uint32_t* grp;
+    uint32_t* tpos;
     __device__ uint64_t load(uint64_t k) const {
         const uint32_t h = head[k];
         const uint32_t nh = (k + 1 < N) ? head[k + 1] : 1u;
@@ -112,6 +114,7 @@ struct OpTied {
             const uint32_t j = (uint32_t)(ex >> 32);
             slot[j] = (uint32_t)k;
             grp[j] = (uint32_t)ex + (uint32_t)v;  // inclusive group number
+            tpos[j] = sa[k];
         }
     }
 };
@@ -170,6 +173,130 @@ struct OpNames {
         uniq[j] = (uint8_t)(v && next_changed);
     }
 };
+
+// Sample records in sample text order (slot k = (p/X)*D + NEXT_RANK[p%X] of
+// sample p): bits [0,32) name, bit 32 unique flag, bits [33,64) index j of the
+// sample in window order.  One random 8-byte write per sample; every later step
+// of phase 3 reads these records with coalesced passes.
+__device__ __forceinline__ uint32_t srec_name(uint64_t r) { return (uint32_t)r; }
+__device__ __forceinline__ uint32_t srec_uniq(uint64_t r) { return (uint32_t)(r >> 32) & 1u; }
+__device__ __forceinline__ uint32_t srec_j(uint64_t r) { return (uint32_t)(r >> 33); }
+
+__global__ void k_scatter_samples(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ name,
+                                  const uint8_t* __restrict__ uniq, const DcFlags* __restrict__ f,
+                                  uint64_t* __restrict__ srec) {
+    const DcFlags& F = *f;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = rank_pos_of(s_pos[j], F);
+        srec[k] = (uint64_t)name[j] | ((uint64_t)uniq[j] << 32) | ((uint64_t)j << 33);
+    }
+}
+
+// Distinct names: the rank of every sample is its name.
+__global__ void k_ranks_from_names(uint64_t m, const uint64_t* __restrict__ srec, uint32_t* __restrict__ rank_text,
+                                   uint32_t* trace_names, uint8_t* trace_uniq) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = srec[k];
+        if (rank_text) rank_text[k] = srec_name(r);
+        if (trace_names) {
+            trace_names[k] = srec_name(r);
+            trace_uniq[k] = (uint8_t)srec_uniq(r);
+        }
+    }
+}
+
+// Recursion string in (mod X, div X) order: position q = samples_before[c] + b
+// holds the name of sample slot k = b*D + c (a transpose of the D-column layout).
+__global__ void k_rec_from_samples(uint64_t m, const uint64_t* __restrict__ srec, const DcFlags* __restrict__ f,
+                                   uint32_t* __restrict__ rec, uint8_t* __restrict__ rec_uniq) {
+    const DcFlags& F = *f;
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = 0;
+        while (c + 1 < F.D && q >= F.samples_before[c + 1]) c++;
+        const uint64_t b = q - F.samples_before[c];
+        const uint64_t r = srec[b * F.D + c];
+        rec[q] = srec_name(r);
+        rec_uniq[q] = (uint8_t)srec_uniq(r);
+    }
+}
+
+// After discarding, unique samples keep their window order: rank = j + 1.
+__global__ void k_ranks_unique_text(uint64_t m, const uint64_t* __restrict__ srec, uint32_t* __restrict__ rank_text) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = srec[k];
+        if (srec_uniq(r)) rank_text[k] = srec_j(r) + 1;
+    }
+}
+
+// Non-unique samples (text order) keyed by (name, rank of their position in the
+// reduced string); value = sample slot k.
+struct OpNonUniqueText {
+    const uint64_t* srec;
+    const DcFlags* f;
+    const uint32_t* kidx;
+    const uint32_t* rank_of;
+    uint32_t* key_lo;
+    uint32_t* key_hi;
+    uint32_t* val;
+    __device__ uint32_t load(uint64_t k) const { return !srec_uniq(srec[k]); }
+    __device__ void store(uint64_t k, uint32_t ex, uint32_t v) const {
+        if (v && key_lo) {  // null outputs: counting pass only
+            const uint64_t b = k / f->D, c = k % f->D;
+            const uint64_t q = f->samples_before[c] + b;
+            key_lo[ex] = rank_of[kidx[q]];
+            key_hi[ex] = srec_name(srec[k]);
+            val[ex] = (uint32_t)k;
+        }
+    }
+};
+
+__global__ void k_ranks_nonunique(uint64_t mu, const uint32_t* __restrict__ key_hi, const uint32_t* __restrict__ val,
+                                  const uint32_t* __restrict__ start_s, const uint32_t* __restrict__ start_l,
+                                  uint32_t* __restrict__ rank_text) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < mu; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t nm = key_hi[t];
+        rank_text[val[t]] = start_s[nm] + (uint32_t)(t - start_l[nm]) + 1;
+    }
+}
+
+// Final SA of a level: sa_full slot 0 is position n (the empty suffix); the
+// n remaining slots are written in 32-, 40- (little endian, high byte 0 since
+// indices are < 2^32) or 64-bit form.  Four entries per thread so the 40-bit
+// form is written as five aligned 32-bit words.
+__global__ void k_emit(const uint32_t* __restrict__ sa_full, uint64_t n, void* __restrict__ out, int width) {
+    const uint64_t groups = n / 4;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t e0 = sa_full[4 * g + 1], e1 = sa_full[4 * g + 2], e2 = sa_full[4 * g + 3], e3 = sa_full[4 * g + 4];
+        if (width == 32) {
+            reinterpret_cast<uint4*>(out)[g] = make_uint4(e0, e1, e2, e3);
+        } else if (width == 64) {
+            ulonglong2* o = reinterpret_cast<ulonglong2*>(out) + 2 * g;
+            o[0] = make_ulonglong2(e0, e1);
+            o[1] = make_ulonglong2(e2, e3);
+        } else {
+            uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * g;
+            o[0] = e0;
+            o[1] = e1 << 8;
+            o[2] = (e1 >> 24) | (e2 << 16);
+            o[3] = (e2 >> 16) | (e3 << 24);
+            o[4] = e3 >> 8;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+        const uint64_t k = groups * 4 + threadIdx.x;
+        const uint32_t v = sa_full[k + 1];
+        if (width == 32) reinterpret_cast<uint32_t*>(out)[k] = v;
+        else if (width == 64) reinterpret_cast<uint64_t*>(out)[k] = v;
+        else {
+            uint8_t* o = reinterpret_cast<uint8_t*>(out) + 5 * k;
+            o[0] = (uint8_t)v;
+            o[1] = (uint8_t)(v >> 8);
+            o[2] = (uint8_t)(v >> 16);
+            o[3] = (uint8_t)(v >> 24);
+            o[4] = 0;
+        }
+    }
+}
 
 // Phase 3 distinct case: ranks = names, scattered to sample text order.
 __global__ void k_scatter_names(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ name,
@@ -324,13 +451,37 @@ __global__ void k_tie_classify(uint64_t G, const uint32_t* __restrict__ starts, 
     if (threadIdx.x < TIE_CLASSES && c[threadIdx.x]) atomicAdd(&counts[threadIdx.x], c[threadIdx.x]);
 }
 
+// Bins tie groups by size class.  Cursor updates are aggregated per warp: the
+// lanes holding the same class elect one lane that reserves their slots.
 __global__ void k_tie_bin(uint64_t G, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
                           uint32_t* __restrict__ cursor, uint32_t* __restrict__ out_start, uint32_t* __restrict__ out_size) {
-    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t sz = ends[g] - starts[g] + 1;
-        const uint32_t slot = atomicAdd(&cursor[tie_class(sz)], 1u);
-        out_start[slot] = starts[g];
-        out_size[slot] = sz;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t first = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t rounds = (G + stride - 1) / stride;
+    for (uint64_t r = 0; r < rounds; r++) {  // every lane runs the same rounds (warp-wide ballots)
+        const uint64_t g = first + r * stride;
+        const bool ok = g < G;
+        uint32_t sz = 0, cls = 31;
+        if (ok) {
+            sz = ends[g] - starts[g] + 1;
+            cls = (uint32_t)tie_class(sz);
+        }
+        uint32_t peers = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const uint32_t bit = (cls >> b) & 1u;
+            const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bal : ~bal;
+        }
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (ok && lane_id() == leader) base = atomicAdd(&cursor[cls], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (ok) {
+            const uint32_t slot = base + __popc(peers & lanemask_lt());
+            out_start[slot] = starts[g];
+            out_size[slot] = sz;
+        }
     }
 }
 

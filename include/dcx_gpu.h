@@ -105,6 +105,10 @@ int dcx_build_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_w
 int dcx_build_sa_strict(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
                         void* sa_out, uint32_t flags);
 
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
+ * caller can time builds with events recorded on it. */
+int dcx_get_stream(dcx_ctx* ctx, void** stream_out);
+
 /* Statistics of the last build on this context. */
 int dcx_get_stats(dcx_ctx* ctx, dcx_stats* out);
 
