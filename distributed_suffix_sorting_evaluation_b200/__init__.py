@@ -48,6 +48,7 @@ EXPORTED = (
     "dcx_ctx_create", "dcx_ctx_destroy", "dcx_set_option", "dcx_build_sa", "dcx_build_sa_strict",
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
+    "dcx_build_sa_noalloc",
 )
 
 
@@ -104,6 +105,7 @@ def load_library(path: str | None = None):
     lib.dcx_strerror.restype = ctypes.c_char_p
     lib.dcx_dc_table.argtypes = [i32, vp, vp, vp, vp]
     lib.dcx_version.restype = ctypes.c_char_p
+    lib.dcx_build_sa_noalloc.argtypes = [vp, u64, vp, vp]
     _lib = lib
     return lib
 

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INC}"]
 HOST_CXX = "/usr/bin/g++"
 
-SOURCES = ["dcx.cu"]
+SOURCES = ["dcx.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "radix.cuh", "keys.cuh", "segsort.cuh", "small_sa.cuh", "level_kernels.cuh"]
 
 

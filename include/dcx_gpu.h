@@ -142,6 +142,21 @@ int dcx_serve_release(dcx_ctx* ctx, uint64_t req_id);
 /* Blocks until every submitted request is done. */
 int dcx_serve_drain(dcx_ctx* ctx);
 
+/* ---- allocation-free entry point ----------------------------------------- */
+/* No counterpart in the reference.  Suffix array of a device-resident text of
+ * at most 32768 bytes, written as uint32 indices to the device buffer sa_dev,
+ * launched on `stream` (a cudaStream_t; 0 = legacy default stream) and
+ * returning without waiting for it.  It never allocates: it is meant for
+ * callers that cannot call cudaMalloc where they need the result (inside stream
+ * capture, inside an allocator, or with all device memory already reserved by
+ * another pool).  All working memory is one 512 KiB device array that every GPU
+ * loading this library holds until the process exits.  The first call on a
+ * device looks that array's address up (cudaGetSymbolAddress) with the device
+ * current, so make it before any stream capture.  Every call reuses the same
+ * array: calls whose kernels overlap on the GPU race, so serialise them (one
+ * stream, or events).  Returns DCX_ERR_ARG for n > 32768 or null pointers. */
+int dcx_build_sa_noalloc(const uint8_t* text_dev, uint64_t n, uint32_t* sa_dev, void* stream);
+
 /* ---- misc ------------------------------------------------------------------ */
 const char* dcx_strerror(int code);
 /* Difference-cover tables generated in closed form (pdcx/difference_cover.hpp):
