@@ -48,7 +48,7 @@ EXPORTED = (
     "dcx_ctx_create", "dcx_ctx_destroy", "dcx_set_option", "dcx_build_sa", "dcx_build_sa_strict",
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
-    "dcx_build_sa_noalloc",
+    "dcx_build_sa_noalloc", "dcx_check_sa",
 )
 
 
@@ -106,6 +106,7 @@ def load_library(path: str | None = None):
     lib.dcx_dc_table.argtypes = [i32, vp, vp, vp, vp]
     lib.dcx_version.restype = ctypes.c_char_p
     lib.dcx_build_sa_noalloc.argtypes = [vp, u64, vp, vp]
+    lib.dcx_check_sa.argtypes = [vp, vp, u64, vp, i32, u32, ctypes.POINTER(i32)]
     _lib = lib
     return lib
 
@@ -192,6 +193,43 @@ class Context:
         flags = DCX_DEVICE_PTRS | (0 if packing else DCX_NO_PACKING)
         _check(self.lib.dcx_build_sa(self.h, ctypes.c_void_p(text_ptr), n, dc, sa_width, ctypes.c_void_p(sa_ptr),
                                      flags))
+
+    def build_sa_batch(self, texts, dc: int = 0, sa_width: int = 32, packing: bool = True):
+        """One SA per text (list of byte strings / uint8 arrays); dc = 0 lets the
+        library choose.  Returns a list of uint64 arrays."""
+        arrs = [np.frombuffer(t, np.uint8) if isinstance(t, (bytes, bytearray)) else np.asarray(t, np.uint8)
+                for t in texts]
+        offs = np.zeros(len(arrs) + 1, np.uint64)
+        offs[1:] = np.cumsum([a.size for a in arrs], dtype=np.uint64)
+        cat = np.ascontiguousarray(np.concatenate(arrs) if arrs else np.zeros(0, np.uint8))
+        wb = sa_dtype_bytes(sa_width)
+        out = np.zeros(max(int(offs[-1]), 1) * wb, np.uint8)
+        flags = DCX_HOST_PTRS | (0 if packing else DCX_NO_PACKING)
+        _check(self.lib.dcx_build_sa_batch(self.h, cat.ctypes.data if cat.size else out.ctypes.data,
+                                           offs.ctypes.data, len(arrs), dc, sa_width, out.ctypes.data, flags))
+        res = []
+        for i, a in enumerate(arrs):
+            b = int(offs[i])
+            res.append(unpack_sa(out[b * wb:(b + a.size) * wb], sa_width, a.size))
+        return res
+
+    def build_sa_batch_raw(self, cat_ptr: int, offs_ptr: int, count: int, out_ptr: int, dc: int = 0,
+                           sa_width: int = 32, device: bool = False):
+        """Batch call on raw pointers (host or device per `device`)."""
+        flags = DCX_DEVICE_PTRS if device else DCX_HOST_PTRS
+        _check(self.lib.dcx_build_sa_batch(self.h, ctypes.c_void_p(cat_ptr), ctypes.c_void_p(offs_ptr), count, dc,
+                                           sa_width, ctypes.c_void_p(out_ptr), flags))
+
+    def check_sa(self, text, sa_raw: np.ndarray, sa_width: int) -> bool:
+        """GPU check that sa_raw (raw bytes, sa_width bits per entry) is the SA of text."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        raw = np.ascontiguousarray(sa_raw).view(np.uint8)
+        ok = ctypes.c_int()
+        _check(self.lib.dcx_check_sa(self.h, t.ctypes.data if t.size else None, t.size,
+                                     raw.ctypes.data if raw.size else None, sa_width, DCX_HOST_PTRS,
+                                     ctypes.byref(ok)))
+        return bool(ok.value)
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""

@@ -187,6 +187,7 @@ struct Options {
     uint32_t prefix_chars = 0;
     int trace = 0;
     uint32_t spin_limit = 1u << 24;
+    uint64_t batch_round_cap = 0;  // max elements per batch round (0 = from the budget)
 };
 
 struct Ctx;
@@ -430,14 +431,35 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
 }
 
 // ---------------------------------------------------------------------------
-// Phase 1: sort all N = n+1 suffixes by their first L chars.  Produces the
-// sorted positions `sa` and head flags (1 where the window differs from the
-// previous one).
+// Texts of one level (host view): text s occupies positions [start[s],
+// start[s+1]-1) of the level buffer, followed by one 0 (its empty suffix).
+// ---------------------------------------------------------------------------
+struct Segs {
+    std::vector<uint64_t> start;  // K + 1 entries, start[K] = N
+    uint32_t K() const { return (uint32_t)start.size() - 1; }
+    uint64_t N() const { return start.back(); }
+    uint64_t len(uint32_t s) const { return start[s + 1] - start[s] - 1; }
+};
+
+template <typename T>
+static DBuf<T> upload(Ctx& c, const std::vector<T>& v) {
+    DBuf<T> d(&c, std::max<size_t>(v.size(), 1));
+    if (!v.empty()) DCX_CUDA(cudaMemcpyAsync(d.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// Phase 1: sort all N suffixes of the level by (text, first L chars).
+// Produces the sorted positions `sa`, head flags (1 where the key differs from
+// the previous one) and, for K > 1, the text id of every sorted element (segw).
 // ---------------------------------------------------------------------------
 template <typename CharT>
-static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint32_t L, int depth,
-                         DBuf<uint32_t>& sa, DBuf<uint8_t>& head) {
-    const uint64_t N = n + 1;
+static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64_t* d_start, uint64_t B, uint32_t L,
+                         int depth, DBuf<uint32_t>& sa, DBuf<uint8_t>& head, DBuf<uint32_t>& segw) {
+    const uint64_t N = sg.N();
+    const uint32_t K = sg.K();
+    const bool SEGK = K > 1;
+    const SegView sv{K, d_start};
     const uint32_t words_full = (key_bits(B, L) + 31) / 32;
     uint32_t kw0_max = depth == 0 ? 2 : 3;
     uint32_t P0 = std::min<uint32_t>(L, max_chars_in(B, std::min(words_full, kw0_max)));
@@ -458,14 +480,15 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
     KeyPlan plan = make_plan(B, P0);
     if (plan.kw > 3) throw Error(DCX_ERR_INTERNAL, "prefix key wider than 3 words");
     const uint32_t kw = plan.kw;
+    const uint32_t kwt = kw + (SEGK ? 1u : 0u);  // + text id word
 
     // round 0
     {
-        DBuf<uint32_t> keys[2][3];
+        DBuf<uint32_t> keys[2][4];
         DBuf<uint32_t> vals[2];
         SortSpace s;
         for (int b = 0; b < 2; b++) {
-            for (uint32_t w = 0; w < kw; w++) {
+            for (uint32_t w = 0; w < kwt; w++) {
                 keys[b][w] = DBuf<uint32_t>(&c, N);
                 s.k[b][w] = keys[b][w].get();
             }
@@ -474,43 +497,56 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
         }
         DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
         KeyOut ko{};
-        for (uint32_t w = 0; w < kw; w++) ko.w[w] = s.k[0][w];
+        for (uint32_t w = 0; w < kwt; w++) ko.w[w] = s.k[0][w];
         const int grid = grid_for(N, 256, 148 * 8);
-        const size_t shm = (size_t)HIST_COPIES * 4 * kw * RADIX * 4;
-        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<1, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
-        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<2, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
-        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<3, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+        const size_t shm = (size_t)HIST_COPIES * 4 * kwt * RADIX * 4;
         if (kw <= 2 && P0 <= (uint32_t)SLIDE_MAX_CHARS) {
             // sliding-window builder: keys of consecutive positions share P-1 chars
             uint64_t pow_top = 1;
             for (uint32_t i = 1; i < P0; i++) pow_top *= B;
             const size_t sshm = keys_slide_smem<CharT>();
-            DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
-            const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 3);
-            k_keys_slide<CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, n, N, plan, pow_top, ko, s.v[0],
-                                                                         c.d_hist);
-        } else if (kw == 1) k_keys_prefix<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
-        else if (kw == 2) k_keys_prefix<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
-        else k_keys_prefix<3, CharT><<<grid, 256, shm, c.stream>>>(text, n, N, plan, ko, s.v[0], c.d_hist);
+            const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 2);
+            if (SEGK) {
+                DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<true, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
+                k_keys_slide<true, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, ko, s.v[0], c.d_hist);
+            } else {
+                DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<false, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
+                k_keys_slide<false, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, ko, s.v[0], c.d_hist);
+            }
+        } else {
+#define DCX_PREFIX(KWV, SEGV)                                                                                       \
+    do {                                                                                                            \
+        DCX_CUDA(cudaFuncSetAttribute(k_keys_prefix<KWV, SEGV, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                      64 << 10));                                                                   \
+        k_keys_prefix<KWV, SEGV, CharT><<<grid, 256, shm, c.stream>>>(text, N, sv, plan, ko, s.v[0], c.d_hist);     \
+    } while (0)
+            if (kw == 1) { if (SEGK) DCX_PREFIX(1, true); else DCX_PREFIX(1, false); }
+            else if (kw == 2) { if (SEGK) DCX_PREFIX(2, true); else DCX_PREFIX(2, false); }
+            else { if (SEGK) DCX_PREFIX(3, true); else DCX_PREFIX(3, false); }
+#undef DCX_PREFIX
+        }
         DCX_CHECK_LAUNCH();
         c.launched();
-        c.alg(N * sizeof(CharT) + N * (kw + 1) * 4);
-        int f = radix_sort(c, kw, N, s);
+        c.alg(N * sizeof(CharT) + N * (kwt + 1) * 4);
+        int f = radix_sort(c, kwt, N, s);
         KeyWords kk{};
-        for (uint32_t w = 0; w < kw; w++) kk.w[w] = s.k[f][w];
+        for (uint32_t w = 0; w < kwt; w++) kk.w[w] = s.k[f][w];
         head = DBuf<uint8_t>(&c, N);
-        k_heads<<<grid_for(N, 256), 256, 0, c.stream>>>(kk, kw, N, head.get());
+        k_heads<<<grid_for(N, 256), 256, 0, c.stream>>>(kk, kwt, N, head.get());
         DCX_CHECK_LAUNCH();
         c.launched();
-        c.alg(N * kw * 4 + N);
+        c.alg(N * kwt * 4 + N);
         sa = std::move(vals[f]);
+        if (SEGK) segw = std::move(keys[f][kwt - 1]);
     }
 
-    // refinement rounds for tied windows
+    // refinement rounds for tied windows (a group never spans two texts)
     uint32_t covered = P0;
     while (covered < L) {
-        DBuf<uint32_t> slot(&c, N), grp(&c, N), tpos(&c, N);
-        OpTied op{head.get(), N, sa.get(), slot.get(), grp.get(), tpos.get()};
+        DBuf<uint32_t> slot(&c, N), grp(&c, N), tpos(&c, N), tseg;
+        if (SEGK) tseg = DBuf<uint32_t>(&c, N);
+        OpTied op{head.get(), N, sa.get(), SEGK ? segw.get() : nullptr, slot.get(), grp.get(), tpos.get(),
+                  SEGK ? tseg.get() : nullptr};
         const uint64_t tot = device_scan<uint64_t>(c, op, N);
         c.alg(N + N / 2);
         const uint64_t cnt = tot >> 32;
@@ -537,11 +573,11 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
         DCX_CUDA(cudaFuncSetAttribute(k_keys_refine<1, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
         DCX_CUDA(cudaFuncSetAttribute(k_keys_refine<2, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
         if (rp.kw == 1)
-            k_keys_refine<1, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, tpos.get(), grp.get(), covered, rp,
-                                                                  ko, s.v[0], c.d_hist);
+            k_keys_refine<1, CharT><<<grid, 256, shm, c.stream>>>(text, sv, cnt, tpos.get(), SEGK ? tseg.get() : nullptr,
+                                                                  grp.get(), covered, rp, ko, s.v[0], c.d_hist);
         else
-            k_keys_refine<2, CharT><<<grid, 256, shm, c.stream>>>(text, n, cnt, tpos.get(), grp.get(), covered, rp,
-                                                                  ko, s.v[0], c.d_hist);
+            k_keys_refine<2, CharT><<<grid, 256, shm, c.stream>>>(text, sv, cnt, tpos.get(), SEGK ? tseg.get() : nullptr,
+                                                                  grp.get(), covered, rp, ko, s.v[0], c.d_hist);
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(cnt * (12 + Pr * sizeof(CharT)) + cnt * (kwr + 1) * 4);
@@ -558,10 +594,10 @@ static void sort_windows(Ctx& c, const CharT* text, uint64_t n, uint64_t B, uint
 }
 
 // ---------------------------------------------------------------------------
-// Phase 4: order every tie group (equal L-char windows) by cover ranks.
+// Phase 4: order every tie group (equal text and L-char window) by cover ranks.
 // ---------------------------------------------------------------------------
 template <int D>
-static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_text, const DcDev* dcd,
+static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_text, const DcDev* dcd, TieSeg ts,
                         const std::vector<uint32_t>& counts, const uint32_t* gstart, const uint32_t* gsize) {
     std::vector<uint64_t> off(TIE_CLASSES + 1, 0);
     for (int k = 0; k < TIE_CLASSES; k++) off[k + 1] = off[k] + counts[k];
@@ -572,7 +608,7 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         const uint64_t warps = div_up(g, 32 / Wv);
         const uint64_t blocks = div_up(warps * 32, 256);
         k_tie_warp<D, Wv><<<(unsigned)blocks, 256, 0, c.stream>>>(gstart + off[cls], gsize + off[cls], (uint32_t)g,
-                                                                  sa, rank_text, dcd);
+                                                                  sa, rank_text, dcd, ts);
         DCX_CHECK_LAUNCH();
         c.launched();
     };
@@ -581,7 +617,7 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
     warp_launch(2, std::integral_constant<int, 8>{});
     warp_launch(3, std::integral_constant<int, 16>{});
     warp_launch(4, std::integral_constant<int, 32>{});
-    auto cta_launch = [&](int cls, const uint32_t* gs, const uint32_t* gz, uint64_t g, auto Cc) {
+    auto cta_launch = [&](const uint32_t* gs, const uint32_t* gz, uint64_t g, auto Cc) {
         constexpr int C = decltype(Cc)::value;
         constexpr int T = C / 2 < 512 ? C / 2 : 512;
         if (!g) return;
@@ -589,18 +625,17 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         DCX_CUDA(cudaFuncSetAttribute(k_tie_cta<D, C, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         for (uint64_t b = 0; b < g; b += 65535ull * 1024) {
             const uint64_t nb = std::min<uint64_t>(g - b, 65535ull * 1024);
-            k_tie_cta<D, C, T><<<(unsigned)nb, T, shm, c.stream>>>(gs + b, gz + b, sa, rank_text, dcd);
+            k_tie_cta<D, C, T><<<(unsigned)nb, T, shm, c.stream>>>(gs + b, gz + b, sa, rank_text, dcd, ts);
             DCX_CHECK_LAUNCH();
             c.launched();
         }
-        (void)cls;
     };
-    cta_launch(5, gstart + off[5], gsize + off[5], counts[5], std::integral_constant<int, 64>{});
-    cta_launch(6, gstart + off[6], gsize + off[6], counts[6], std::integral_constant<int, 128>{});
-    cta_launch(7, gstart + off[7], gsize + off[7], counts[7], std::integral_constant<int, 256>{});
-    cta_launch(8, gstart + off[8], gsize + off[8], counts[8], std::integral_constant<int, 512>{});
-    cta_launch(9, gstart + off[9], gsize + off[9], counts[9], std::integral_constant<int, 1024>{});
-    cta_launch(10, gstart + off[10], gsize + off[10], counts[10], std::integral_constant<int, 2048>{});
+    cta_launch(gstart + off[5], gsize + off[5], counts[5], std::integral_constant<int, 64>{});
+    cta_launch(gstart + off[6], gsize + off[6], counts[6], std::integral_constant<int, 128>{});
+    cta_launch(gstart + off[7], gsize + off[7], counts[7], std::integral_constant<int, 256>{});
+    cta_launch(gstart + off[8], gsize + off[8], counts[8], std::integral_constant<int, 512>{});
+    cta_launch(gstart + off[9], gsize + off[9], counts[9], std::integral_constant<int, 1024>{});
+    cta_launch(gstart + off[10], gsize + off[10], counts[10], std::integral_constant<int, 2048>{});
     const uint64_t nbig = counts[11];
     if (!nbig) return;
     // big groups: sort 2048-chunks, then merge rounds
@@ -619,20 +654,16 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         offs[g + 1] = offs[g] + bsize[g];
         maxsz = std::max(maxsz, bsize[g]);
     }
-    DBuf<uint32_t> dcs(&c, cstart.size()), dcz(&c, csize.size()), dbs(&c, nbig);
-    DBuf<uint64_t> doff(&c, nbig + 1);
-    DCX_CUDA(cudaMemcpyAsync(dcs.get(), cstart.data(), cstart.size() * 4, cudaMemcpyHostToDevice, c.stream));
-    DCX_CUDA(cudaMemcpyAsync(dcz.get(), csize.data(), csize.size() * 4, cudaMemcpyHostToDevice, c.stream));
-    DCX_CUDA(cudaMemcpyAsync(dbs.get(), bstart.data(), nbig * 4, cudaMemcpyHostToDevice, c.stream));
-    DCX_CUDA(cudaMemcpyAsync(doff.get(), offs.data(), (nbig + 1) * 8, cudaMemcpyHostToDevice, c.stream));
-    cta_launch(11, dcs.get(), dcz.get(), cstart.size(), std::integral_constant<int, 2048>{});
+    DBuf<uint32_t> dcs = upload(c, cstart), dcz = upload(c, csize), dbs = upload(c, bstart);
+    DBuf<uint64_t> doff = upload(c, offs);
+    cta_launch(dcs.get(), dcz.get(), cstart.size(), std::integral_constant<int, 2048>{});
     DBuf<uint32_t> tmp(&c, N);
     uint32_t* src = sa;
     uint32_t* dst = tmp.get();
     const uint64_t total = offs[nbig];
     for (uint64_t w = 2048; w < maxsz; w <<= 1) {
         k_tie_merge<D><<<grid_for(total, 256), 256, 0, c.stream>>>(doff.get(), (uint32_t)nbig, dbs.get(), total,
-                                                                   (uint32_t)w, src, dst, rank_text, dcd);
+                                                                   (uint32_t)w, src, dst, rank_text, dcd, ts);
         DCX_CHECK_LAUNCH();
         c.launched();
         std::swap(src, dst);
@@ -646,7 +677,7 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
 }
 
 static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, const uint32_t* rank_text,
-                      const DcHost& dc) {
+                      const DcHost& dc, TieSeg ts) {
     DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1);
     OpGroups op{head, N, starts.get(), ends.get()};
     const uint64_t tot = device_scan<uint64_t>(c, op, N);
@@ -676,43 +707,49 @@ static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, con
     ends.reset();
     const DcDev* dcd = c.dc_dev[dc.X];
     switch (dc.D) {
-        case 2: tie_break_d<2>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 3: tie_break_d<3>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 4: tie_break_d<4>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 5: tie_break_d<5>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 6: tie_break_d<6>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 7: tie_break_d<7>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 8: tie_break_d<8>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 9: tie_break_d<9>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 10: tie_break_d<10>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 11: tie_break_d<11>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
-        case 12: tie_break_d<12>(c, sa, N, rank_text, dcd, counts, gstart.get(), gsize.get()); break;
+#define DCX_TIE(DV) \
+    case DV: tie_break_d<DV>(c, sa, N, rank_text, dcd, ts, counts, gstart.get(), gsize.get()); break;
+        DCX_TIE(2) DCX_TIE(3) DCX_TIE(4) DCX_TIE(5) DCX_TIE(6) DCX_TIE(7) DCX_TIE(8) DCX_TIE(9) DCX_TIE(10)
+        DCX_TIE(11) DCX_TIE(12)
+#undef DCX_TIE
         default: throw Error(DCX_ERR_INTERNAL, "unsupported D");
     }
     c.st.tie_groups += G;
 }
 
 // ---------------------------------------------------------------------------
-// One DCX level.  text: device chars in 1..sigma, length n.  sa_out: n entries.
+// One DCX level over K texts.
 // ---------------------------------------------------------------------------
-struct LevelInfo {
-    uint32_t sample_chars;
-};
-
 template <typename CharT>
-static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_t X, int depth, bool packing,
+static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uint32_t X, int depth, bool packing,
                   void* sa_out, int out_width = 32);
 
-static void small_sa_single(Ctx& c, const void* text, bool wide, uint64_t n, uint32_t* sa_out) {
-    uint64_t offs[2] = {0, n};
-    DBuf<uint64_t> d(&c, 2);
-    DCX_CUDA(cudaMemcpyAsync(d.get(), offs, 16, cudaMemcpyHostToDevice, c.stream));
-    if (wide)
-        k_small_sa<uint32_t><<<1, SMALL_THREADS, 0, c.stream>>>((const uint32_t*)text, d.get(), nullptr, sa_out);
-    else
-        k_small_sa<uint8_t><<<1, SMALL_THREADS, 0, c.stream>>>((const uint8_t*)text, d.get(), nullptr, sa_out);
-    DCX_CHECK_LAUNCH();
-    c.launched();
+// In-CTA base case for K texts of at most SMALL_MAX chars each (one launch).
+static void small_sa_batch(Ctx& c, const void* text, bool wide, const Segs& sg, void* out, int out_width) {
+    const uint32_t K = sg.K();
+    std::vector<uint64_t> obase(K + 1, 0);
+    for (uint32_t s = 0; s < K; s++) obase[s + 1] = obase[s] + sg.len(s);
+    DBuf<uint64_t> dst = upload(c, sg.start), dob = upload(c, obase);
+    DBuf<uint32_t> tmp;
+    uint32_t* o32 = (uint32_t*)out;
+    if (out_width != 32) {
+        tmp = DBuf<uint32_t>(&c, std::max<uint64_t>(obase[K], 1));
+        o32 = tmp.get();
+    }
+    for (uint32_t b = 0; b < K; b += 65535) {
+        const uint32_t nb = std::min<uint32_t>(K - b, 65535);
+        if (wide)
+            k_small_sa<uint32_t><<<nb, SMALL_THREADS, 0, c.stream>>>((const uint32_t*)text, dst.get() + b, dob.get() + b, o32);
+        else
+            k_small_sa<uint8_t><<<nb, SMALL_THREADS, 0, c.stream>>>((const uint8_t*)text, dst.get() + b, dob.get() + b, o32);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    }
+    if (out_width != 32) {
+        k_widen<<<grid_for(obase[K], 256), 256, 0, c.stream>>>(o32, obase[K], (uint8_t*)out, out_width);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    }
     DCX_CUDA(cudaStreamSynchronize(c.stream));
 }
 
@@ -728,34 +765,48 @@ static uint32_t level0_sample_chars(uint32_t X, uint64_t sigma, bool packing) {
 }
 
 template <typename CharT>
-static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_t X, int depth, bool packing,
+static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uint32_t X, int depth, bool packing,
                   void* sa_out, int out_width) {
-    if (n == 0) return;
+    const uint32_t K = sg.K();
+    const uint64_t N = sg.N();
+    if (N <= K) return;  // only empty texts
     if (depth > 64) throw Error(DCX_ERR_INTERNAL, "recursion deeper than 64 levels");
     c.st.levels = std::max<uint32_t>(c.st.levels, (uint32_t)depth + 1);
-    if (n <= c.opt.small_threshold && n <= (uint64_t)SMALL_MAX) {
-        if (out_width == 32) {
-            small_sa_single(c, text, sizeof(CharT) == 4, n, (uint32_t*)sa_out);
-        } else {
-            DBuf<uint32_t> tmp(&c, n);
-            small_sa_single(c, text, sizeof(CharT) == 4, n, tmp.get());
-            k_widen<<<grid_for(n, 256), 256, 0, c.stream>>>(tmp.get(), n, (uint8_t*)sa_out, out_width);
-            DCX_CHECK_LAUNCH();
-            c.launched();
-            DCX_CUDA(cudaStreamSynchronize(c.stream));
+    {
+        uint64_t maxlen = 0;
+        for (uint32_t s = 0; s < K; s++) maxlen = std::max(maxlen, sg.len(s));
+        if (maxlen <= c.opt.small_threshold && maxlen <= (uint64_t)SMALL_MAX) {
+            small_sa_batch(c, text, sizeof(CharT) == 4, sg, sa_out, out_width);
+            return;
         }
-        return;
     }
     const DcHost& dc = get_dc(c, X);
     const uint32_t D = dc.D;
     const uint32_t L = depth == 0 ? level0_sample_chars(X, sigma, packing) : X;
     const uint64_t B = sigma + 1;
-    const uint64_t N = n + 1;
-    const uint64_t rem = n % X;
-    const bool dummy = dc.in_dc[rem] != 0;
-    uint64_t m = (n / X) * D;
-    for (uint64_t r = 0; r < rem; r++) m += dc.in_dc[r];
-    m += dummy;
+
+    // ---- phase 0: per-text lengths, samples, slot bases (pdcx.hpp:473-510)
+    std::vector<uint64_t> m_s(K), rbase(K + 1, 0), qbase(K + 1, 0), obase(K + 1, 0), sbt((size_t)K * (D + 1), 0);
+    std::vector<uint64_t> num_at_mod(X);
+    for (uint32_t s = 0; s < K; s++) {
+        const uint64_t n = sg.len(s);
+        const uint64_t rem = n % X;
+        const bool dummy = dc.in_dc[rem] != 0;
+        uint64_t m = (n / X) * D;
+        for (uint64_t r = 0; r < rem; r++) m += dc.in_dc[r];
+        m += dummy;
+        m_s[s] = m;
+        for (uint64_t i = 0; i < X; i++) num_at_mod[i] = (n + X - 1 - i) / X;
+        num_at_mod[rem] += dummy;
+        uint64_t* sb = &sbt[(size_t)s * (D + 1)];
+        for (uint32_t i = 1; i <= D; i++) sb[i] = sb[i - 1] + num_at_mod[dc.dc[i - 1]];
+        rbase[s + 1] = rbase[s] + m + D;
+        qbase[s + 1] = qbase[s] + m;
+        obase[s + 1] = obase[s] + n;
+    }
+    const uint64_t m = qbase[K];
+    const uint64_t slots = rbase[K];
+    if (m >= (1ull << 31)) throw Error(DCX_ERR_ARG, "more than 2^31 samples in one level");
     DcFlags fl{};
     fl.X = X;
     fl.D = D;
@@ -764,32 +815,31 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
         fl.next_rank[i] = dc.next_rank[i];
     }
     for (uint32_t i = 0; i < D; i++) fl.dc[i] = dc.dc[i];
-    {
-        std::vector<uint64_t> num_at_mod(X);
-        for (uint64_t i = 0; i < X; i++) num_at_mod[i] = (n + X - 1 - i) / X;
-        num_at_mod[rem] += dummy;
-        fl.samples_before[0] = 0;
-        for (uint32_t i = 1; i <= D; i++) fl.samples_before[i] = fl.samples_before[i - 1] + num_at_mod[dc.dc[i - 1]];
-    }
     DBuf<DcFlags> dfl(&c, 1);
     DCX_CUDA(cudaMemcpyAsync(dfl.get(), &fl, sizeof(fl), cudaMemcpyHostToDevice, c.stream));
+    DBuf<uint64_t> d_start = upload(c, sg.start), d_rbase = upload(c, rbase), d_qbase = upload(c, qbase),
+                   d_obase = upload(c, obase), d_sb = upload(c, sbt);
+    DBuf<uint8_t> d_mode(&c, K);
+    DBuf<uint64_t> d_kbase(&c, K + 1), d_start2(&c, K);
+    LevelSeg ls{K, d_start.get(), d_rbase.get(), d_qbase.get(), d_sb.get(), d_obase.get(), d_mode.get(),
+                d_kbase.get(), d_start2.get()};
 
     cudaEvent_t ev[5];
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], c.stream);
 
     // ---- phase 1: window sort
-    DBuf<uint32_t> sa;
+    DBuf<uint32_t> sa, segw;
     DBuf<uint8_t> head;
-    sort_windows<CharT>(c, text, n, B, L, depth, sa, head);
+    sort_windows<CharT>(c, text, sg, d_start.get(), B, L, depth, sa, head, segw);
+    const uint32_t* segw_p = K > 1 ? segw.get() : nullptr;
 
     // ---- phase 2: names
-    if (m >= (1ull << 31)) throw Error(DCX_ERR_ARG, "more than 2^31 samples in one level");
-    DBuf<uint32_t> s_pos(&c, m), s_grp(&c, m);
+    DBuf<uint32_t> s_pos(&c, m), s_seg(&c, m), s_grp(&c, m);
     {
-        OpSamples op{head.get(), sa.get(), dfl.get(), s_pos.get(), s_grp.get(), m};
+        OpSamples op{head.get(), sa.get(), segw_p, dfl.get(), ls, s_pos.get(), s_seg.get(), s_grp.get(), m};
         const uint64_t tot = device_scan<uint64_t>(c, op, N);
-        c.alg(N * 5 + m * 8);
+        c.alg(N * 5 + m * 12);
         if ((tot >> 32) != m) throw Error(DCX_ERR_INTERNAL, "sample count mismatch");
     }
     DBuf<uint32_t> name(&c, m);
@@ -802,23 +852,25 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
     s_grp.reset();
     const uint32_t last_rank = d2h_scalar(c, name.get() + (m - 1));
     // sample records in sample text order (one random scatter)
-    DBuf<uint64_t> srec(&c, m);
-    k_scatter_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), name.get(), uniq.get(), dfl.get(),
-                                                             srec.get());
+    DBuf<uint64_t> srec(&c, slots);
+    DCX_CUDA(cudaMemsetAsync(srec.get(), 0xff, slots * 8, c.stream));
+    k_scatter_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), s_seg.get(), name.get(), uniq.get(),
+                                                             dfl.get(), ls, srec.get());
     DCX_CHECK_LAUNCH();
     c.launched();
-    c.alg(m * 17);
+    c.alg(m * 21);
     s_pos.reset();
+    s_seg.reset();
     uniq.reset();
     if (depth == 0) {
         c.st.level0_samples = m;
         c.st.level0_last_rank = last_rank;
         c.st.level0_recursion = 0;
         c.st.level0_reduction = 0;
-        if (c.opt.trace) {
-            DBuf<uint32_t> tn(&c, m);
-            DBuf<uint8_t> tu(&c, m);
-            k_ranks_from_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), nullptr, tn.get(), tu.get());
+        if (c.opt.trace && K == 1) {
+            DBuf<uint32_t> tn(&c, slots);
+            DBuf<uint8_t> tu(&c, slots);
+            k_ranks_from_names<<<grid_for(slots, 256), 256, 0, c.stream>>>(slots, srec.get(), nullptr, tn.get(), tu.get());
             DCX_CHECK_LAUNCH();
             c.trace_names.resize(m);
             c.trace_uniq.resize(m);
@@ -829,122 +881,166 @@ static void level(Ctx& c, const CharT* text, uint64_t n, uint64_t sigma, uint32_
     }
     cudaEventRecord(ev[1], c.stream);
 
-    // ---- phase 3: ranks of the samples in sample text order, D zero slots of padding
-    DBuf<uint32_t> rank_text(&c, m + D);
-    DCX_CUDA(cudaMemsetAsync(rank_text.get() + m, 0, D * 4, c.stream));
-    if (last_rank >= m) {
+    // ---- phase 3: ranks of the samples in sample text order (D zero slots per text)
+    DBuf<uint32_t> rank_text(&c, slots);
+    DCX_CUDA(cudaMemsetAsync(rank_text.get(), 0, slots * 4, c.stream));
+    if (last_rank >= m) {  // every text's names are distinct (pdcx.hpp:743-757)
         name.reset();
-        k_ranks_from_names<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), rank_text.get(), nullptr, nullptr);
+        k_ranks_from_names<<<grid_for(slots, 256), 256, 0, c.stream>>>(slots, srec.get(), rank_text.get(), nullptr, nullptr);
         DCX_CHECK_LAUNCH();
         c.launched();
-        c.alg(m * 12);
+        c.alg(slots * 12);
     } else {
         const uint32_t Xr = c.opt.recursion_dc ? c.opt.recursion_dc : X;
-        DBuf<uint32_t> rec(&c, m);
-        DBuf<uint8_t> rec_uniq(&c, m);
-        k_rec_from_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), dfl.get(), rec.get(), rec_uniq.get());
+        DBuf<uint32_t> rec(&c, m), kidx(&c, m);
+        DBuf<uint8_t> rec_flag(&c, m);
+        k_rec_from_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), dfl.get(), ls, rec.get(),
+                                                                  rec_flag.get());
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(m * 13);
-        // discarding decision (pdcx.hpp:150-165)
-        DBuf<uint32_t> kidx(&c, m);
-        OpKeep kop{rec_uniq.get(), rec.get(), nullptr, kidx.get()};
-        const uint32_t after = device_scan<uint32_t>(c, kop, m);
+        // per-text discarding counts (num_ranks_after_discarding, pdcx.hpp:215-228)
+        const uint32_t kept_total = device_scan<uint32_t>(c, OpKeepCount{rec_flag.get(), kidx.get()}, m);
         c.alg(m * 6);
-        const double reduction = (double)after / (double)m;
-        const bool discard = reduction <= c.opt.discarding_threshold;
-        if (depth == 0) {
-            c.st.level0_recursion = discard ? 2 : 1;
-            c.st.level0_reduction = reduction;
+        std::vector<uint32_t> kb(K + 1);
+        {
+            DBuf<uint32_t> dkb(&c, K + 1);
+            k_gather_u32<<<grid_for(K + 1, 256), 256, 0, c.stream>>>(kidx.get(), d_qbase.get(), K + 1, m, kept_total,
+                                                                    dkb.get());
+            DCX_CHECK_LAUNCH();
+            DCX_CUDA(cudaMemcpyAsync(kb.data(), dkb.get(), (K + 1) * 4, cudaMemcpyDeviceToHost, c.stream));
+            DCX_CUDA(cudaStreamSynchronize(c.stream));
         }
-        if (!discard) {
-            kidx.reset();
-            rec_uniq.reset();
-            srec.reset();
-            name.reset();
-            DBuf<uint32_t> sa_r(&c, m);
-            level<uint32_t>(c, rec.get(), m, last_rank, Xr, depth + 1, false, sa_r.get());
-            rec.reset();
-            k_ranks_from_rec<<<grid_for(m, 256), 256, 0, c.stream>>>(m, sa_r.get(), dfl.get(), rank_text.get());
-            DCX_CHECK_LAUNCH();
-            c.launched();
-            c.alg(m * 8);
-        } else {
-            DBuf<uint32_t> rec2(&c, after);
-            OpKeep kop2{rec_uniq.get(), rec.get(), rec2.get(), nullptr};
-            device_scan<uint32_t>(c, kop2, m);
-            c.alg(m * 6 + after * 4);
-            rec.reset();
-            rec_uniq.reset();
-            DBuf<uint32_t> sa2(&c, after);
-            level<uint32_t>(c, rec2.get(), after, last_rank, Xr, depth + 1, false, sa2.get());
-            rec2.reset();
-            DBuf<uint32_t> rank_of(&c, after);
-            k_inverse<<<grid_for(after, 256), 256, 0, c.stream>>>(after, sa2.get(), rank_of.get());
-            DCX_CHECK_LAUNCH();
-            c.launched();
-            sa2.reset();
-            // unique samples keep their window order
-            k_ranks_unique_text<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), rank_text.get());
-            DCX_CHECK_LAUNCH();
-            c.launched();
-            c.alg(m * 12);
-            // non-unique samples keyed by (name, rank2) (pdcx.hpp:296-346)
-            const uint64_t mu_cap = m - 0;  // upper bound
-            DBuf<uint32_t> keys[2][2];
-            DBuf<uint32_t> vals[2];
-            SortSpace s;
-            const uint32_t mu = device_scan<uint32_t>(
-                c, OpNonUniqueText{srec.get(), dfl.get(), kidx.get(), rank_of.get(), nullptr, nullptr, nullptr}, m);
-            (void)mu_cap;
-            if (mu) {
-                for (int bb = 0; bb < 2; bb++) {
-                    for (int w = 0; w < 2; w++) {
-                        keys[bb][w] = DBuf<uint32_t>(&c, mu);
-                        s.k[bb][w] = keys[bb][w].get();
-                    }
-                    vals[bb] = DBuf<uint32_t>(&c, mu);
-                    s.v[bb] = vals[bb].get();
+        // per text: recursion iff some name repeats (then more than the first element is
+        // kept); discarding iff the reduction <= threshold (pdcx.hpp:150-165)
+        std::vector<uint8_t> mode(K);
+        std::vector<uint64_t> kbase(K + 1, 0), start2(K, 0);
+        std::vector<uint64_t> rec_start(1, 0);
+        std::vector<uint32_t> rec_text;
+        uint64_t pos2 = 0;
+        for (uint32_t s = 0; s < K; s++) {
+            const uint64_t cnt = kb[s + 1] - kb[s];
+            uint64_t kept = 0;
+            if (cnt >= 2) {
+                const double reduction = (double)cnt / (double)m_s[s];
+                const bool discard = reduction <= c.opt.discarding_threshold;
+                mode[s] = discard ? REC_DISCARD : REC_DIRECT;
+                kept = discard ? cnt : m_s[s];
+                if (depth == 0 && K == 1) {
+                    c.st.level0_recursion = discard ? 2 : 1;
+                    c.st.level0_reduction = reduction;
                 }
-                OpNonUniqueText nop{srec.get(), dfl.get(), kidx.get(), rank_of.get(), s.k[0][0], s.k[0][1], s.v[0]};
-                device_scan<uint32_t>(c, nop, m);
-                c.alg(m * 9 + mu * 24);
-                rank_of.reset();
-                kidx.reset();
-                DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
-                SortPassArgs ha{};
-                ha.keys_in[0] = s.k[0][0];
-                ha.keys_in[1] = s.k[0][1];
-                ha.kw = 2;
-                ha.n = mu;
-                k_digit_hist<<<grid_for(mu, 256, 148 * 4), 256, 8 * RADIX * 4, c.stream>>>(ha, c.d_hist);
-                DCX_CHECK_LAUNCH();
-                c.launched();
-                c.alg(mu * 8);
-                int f = radix_sort(c, 2, mu, s);
-                DBuf<uint32_t> start_s(&c, (uint64_t)last_rank + 1), start_l(&c, (uint64_t)last_rank + 1);
-                k_name_starts<<<grid_for(m, 256), 256, 0, c.stream>>>(m, name.get(), start_s.get());
-                k_name_starts<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], start_l.get());
-                k_ranks_nonunique<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], s.v[f], start_s.get(),
-                                                                          start_l.get(), rank_text.get());
-                DCX_CHECK_LAUNCH();
-                c.launched(3);
-                c.alg(m * 8 + mu * 8 + mu * 24);
+            } else {
+                mode[s] = REC_NONE;
+            }
+            kbase[s + 1] = kbase[s] + kept;
+            if (kept) {
+                start2[s] = pos2;
+                pos2 += kept + 1;
+                rec_start.push_back(pos2);
+                rec_text.push_back(s);
             }
         }
+        DCX_CUDA(cudaMemcpyAsync(d_mode.get(), mode.data(), K, cudaMemcpyHostToDevice, c.stream));
+        DCX_CUDA(cudaMemcpyAsync(d_kbase.get(), kbase.data(), (K + 1) * 8, cudaMemcpyHostToDevice, c.stream));
+        DCX_CUDA(cudaMemcpyAsync(d_start2.get(), start2.data(), K * 8, cudaMemcpyHostToDevice, c.stream));
+        const uint32_t R = (uint32_t)rec_text.size();
+        const uint64_t total2 = kbase[K];
+        bool any_discard = false;
+        for (uint32_t s = 0; s < K; s++) any_discard |= mode[s] == REC_DISCARD;
+        if (R > 0) {
+            // recursion input: the kept names of every recursing text, each followed by a 0
+            DBuf<uint32_t> rec2(&c, pos2);
+            DCX_CUDA(cudaMemsetAsync(rec2.get(), 0, pos2 * 4, c.stream));
+            device_scan<uint32_t>(c, OpCompact{rec_flag.get(), rec.get(), ls, rec2.get(), kidx.get()}, m);
+            c.alg(m * 10 + total2 * 4);
+            rec.reset();
+            rec_flag.reset();
+            Segs sg2;
+            sg2.start = rec_start;
+            DBuf<uint32_t> sa2(&c, total2);
+            level<uint32_t>(c, rec2.get(), sg2, last_rank, Xr, depth + 1, false, sa2.get(), 32);
+            rec2.reset();
+            std::vector<uint64_t> o2(R + 1, 0);
+            for (uint32_t r = 0; r < R; r++) o2[r + 1] = o2[r] + sg2.len(r);
+            DBuf<uint64_t> d_o2 = upload(c, o2);
+            DBuf<uint32_t> d_rt = upload(c, rec_text);
+            DBuf<uint32_t> rank_of;
+            if (any_discard) rank_of = DBuf<uint32_t>(&c, total2);
+            k_after_recursion<<<grid_for(total2, 256), 256, 0, c.stream>>>(total2, sa2.get(), d_o2.get(), R,
+                                                                           d_rt.get(), dfl.get(), ls, rank_text.get(),
+                                                                           any_discard ? rank_of.get() : nullptr);
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            c.alg(total2 * 12);
+            sa2.reset();
+            if (any_discard) {
+                // non-unique samples of discarding texts: sort by (name, rank2) (pdcx.hpp:296-346)
+                const uint32_t mu = device_scan<uint32_t>(
+                    c, OpNonUniqueSeg{srec.get(), dfl.get(), ls, kidx.get(), rank_of.get(), nullptr, nullptr, nullptr},
+                    slots);
+                if (mu) {
+                    DBuf<uint32_t> keys[2][2];
+                    DBuf<uint32_t> vals[2];
+                    SortSpace s;
+                    for (int bb = 0; bb < 2; bb++) {
+                        for (int w = 0; w < 2; w++) {
+                            keys[bb][w] = DBuf<uint32_t>(&c, mu);
+                            s.k[bb][w] = keys[bb][w].get();
+                        }
+                        vals[bb] = DBuf<uint32_t>(&c, mu);
+                        s.v[bb] = vals[bb].get();
+                    }
+                    device_scan<uint32_t>(c, OpNonUniqueSeg{srec.get(), dfl.get(), ls, kidx.get(), rank_of.get(),
+                                                            s.k[0][0], s.k[0][1], s.v[0]},
+                                          slots);
+                    c.alg(slots * 9 + mu * 24);
+                    rank_of.reset();
+                    kidx.reset();
+                    DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+                    SortPassArgs ha{};
+                    ha.keys_in[0] = s.k[0][0];
+                    ha.keys_in[1] = s.k[0][1];
+                    ha.kw = 2;
+                    ha.n = mu;
+                    k_digit_hist<<<grid_for(mu, 256, 148 * 4), 256, 8 * RADIX * 4, c.stream>>>(ha, c.d_hist);
+                    DCX_CHECK_LAUNCH();
+                    c.launched();
+                    c.alg(mu * 8);
+                    int f = radix_sort(c, 2, mu, s);
+                    DBuf<uint32_t> start_s(&c, (uint64_t)last_rank + 1), start_l(&c, (uint64_t)last_rank + 1);
+                    k_name_starts<<<grid_for(m, 256), 256, 0, c.stream>>>(m, name.get(), start_s.get());
+                    k_name_starts<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], start_l.get());
+                    k_ranks_nonunique<<<grid_for(mu, 256), 256, 0, c.stream>>>(mu, s.k[f][1], s.v[f], start_s.get(),
+                                                                              start_l.get(), rank_text.get());
+                    DCX_CHECK_LAUNCH();
+                    c.launched(3);
+                    c.alg(m * 8 + mu * 8 + mu * 24);
+                }
+            }
+        }
+        // texts without recursion keep their names; unique samples of discarding texts their order
+        k_ranks_rest<<<grid_for(slots, 256), 256, 0, c.stream>>>(slots, srec.get(), ls, rank_text.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(slots * 12);
     }
     srec.reset();
     name.reset();
     cudaEventRecord(ev[2], c.stream);
 
     // ---- phase 4: tie groups, then emit
-    tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc);
+    tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc, TieSeg{segw_p, d_start.get(), d_rbase.get()});
     head.reset();
     rank_text.reset();
-    k_emit<<<grid_for(n / 4 + 1, 256), 256, 0, c.stream>>>(sa.get(), n, sa_out, out_width);
+    if (K == 1) {
+        k_emit<<<grid_for(N / 4 + 1, 256), 256, 0, c.stream>>>(sa.get(), N - 1, sa_out, out_width);
+    } else {
+        k_emit_seg<<<grid_for(N, 256), 256, 0, c.stream>>>(sa.get(), segw.get(), N, ls, sa_out, out_width);
+    }
     DCX_CHECK_LAUNCH();
     c.launched();
-    c.alg(n * (4 + out_width / 8));
+    c.alg(N * (4 + out_width / 8));
     cudaEventRecord(ev[3], c.stream);
     DCX_CUDA(cudaEventSynchronize(ev[3]));
     if (depth == 0) {
@@ -1043,6 +1139,9 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     c.alg(n * 3);
     c.st.sigma = (uint32_t)sigma;
     cudaEventRecord(e2, c.stream);
+    Segs one;  // the text as the only segment of level 0, followed by its 0
+    one.start = {0, n + 1};
+    DCX_CUDA(cudaMemsetAsync(t_map.get() + n, 0, 16, c.stream));
     // SA straight into the caller's device buffer, or into a staging buffer for host pointers
     const size_t wb = width / 8;
     DBuf<uint8_t> stage;
@@ -1054,16 +1153,17 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     if (wide_text) {
         // all 256 byte values occur: remap b -> b + 1 into 32-bit chars and build
         // with 257-symbol keys (the reference cli refuses this input)
-        DBuf<uint32_t> t32(&c, n);
+        DBuf<uint32_t> t32(&c, n + 1);
+        DCX_CUDA(cudaMemsetAsync(t32.get() + n, 0, 4, c.stream));
         k_widen_text<<<grid_for(n, 256), 256, 0, c.stream>>>(dtext, n, t32.get());
         DCX_CHECK_LAUNCH();
         c.launched();
         t_in.reset();
         t_map.reset();
-        level<uint32_t>(c, t32.get(), n, sigma, (uint32_t)X, 0, packing, dout, width);
+        level<uint32_t>(c, t32.get(), one, sigma, (uint32_t)X, 0, packing, dout, width);
     } else {
         t_in.reset();
-        level<uint8_t>(c, t_map.get(), n, sigma, (uint32_t)X, 0, packing, dout, width);
+        level<uint8_t>(c, t_map.get(), one, sigma, (uint32_t)X, 0, packing, dout, width);
     }
     t_map.reset();
     if (dev && dout != sa_out)
@@ -1090,6 +1190,191 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
     cudaEventDestroy(e3);
+}
+
+// ---------------------------------------------------------------------------
+// Batch: one SA per text.  Texts of at most SMALL_MAX chars are solved together
+// by the in-CTA base case (one launch); the others run through segmented DCX
+// levels, as many texts per round as the memory budget allows.  The alphabet
+// remap of a round is the union of its texts' alphabets, which keeps every
+// text's order (and therefore its SA) unchanged.
+// ---------------------------------------------------------------------------
+static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, uint32_t K, int dc_or_auto, int width,
+                        void* sa_out, uint32_t flags) {
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (K == 0) return;
+    if (!offsets || !texts || !sa_out) throw Error(DCX_ERR_ARG, "null pointer");
+    const uint32_t X = dc_or_auto == 0 ? 39u : (uint32_t)dc_or_auto;  // auto: DC39 for every DCX-sized text
+    get_dc(c, X);
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    const bool packing = !(flags & DCX_NO_PACKING);
+    const size_t wb = width / 8;
+    for (uint32_t s = 0; s < K; s++) {
+        if (offsets[s + 1] < offsets[s]) throw Error(DCX_ERR_ARG, "offsets must be non-decreasing");
+        if (offsets[s + 1] - offsets[s] >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    }
+    c.st = dcx_stats{};
+    c.peak = c.in_use;
+    const uint64_t base0 = offsets[0];
+    // rounds: consecutive texts whose total stays below the per-round element cap
+    const uint64_t budget_left = c.budget > c.in_use ? c.budget - c.in_use : 0;
+    uint64_t cap = std::min<uint64_t>(1ull << 30, std::max<uint64_t>(budget_left / 48, 1ull << 20));
+    if (c.opt.batch_round_cap) cap = c.opt.batch_round_cap;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c.stream);
+    uint32_t s0 = 0;
+    while (s0 < K) {
+        uint32_t s1 = s0;
+        uint64_t tot = 0;
+        while (s1 < K && (s1 == s0 || tot + (offsets[s1 + 1] - offsets[s1] + 1) <= cap)) {
+            tot += offsets[s1 + 1] - offsets[s1] + 1;
+            s1++;
+        }
+        const uint32_t Kr = s1 - s0;
+        const uint64_t in_bytes = offsets[s1] - offsets[s0];
+        // input of the round on the device (one copy)
+        DBuf<uint8_t> din;
+        const uint8_t* dsrc = texts + (offsets[s0] - base0);
+        if (!dev) {
+            din = DBuf<uint8_t>(&c, in_bytes + 16);
+            if (in_bytes) DCX_CUDA(cudaMemcpyAsync(din.get(), dsrc, in_bytes, cudaMemcpyHostToDevice, c.stream));
+            dsrc = din.get();
+        }
+        // alphabet of the round
+        unsigned long long h[256];
+        DCX_CUDA(cudaMemsetAsync(c.d_h256, 0, 256 * 8, c.stream));
+        if (in_bytes) {
+            if ((uintptr_t)dsrc & 15) {
+                DBuf<uint8_t> al(&c, in_bytes + 16);
+                DCX_CUDA(cudaMemcpyAsync(al.get(), dsrc, in_bytes, cudaMemcpyDeviceToDevice, c.stream));
+                k_hist256<<<grid_for(in_bytes / 16 + 1, 256, 148 * 4), 256, 0, c.stream>>>(al.get(), in_bytes, c.d_h256);
+                DCX_CHECK_LAUNCH();
+                DCX_CUDA(cudaMemcpyAsync(h, c.d_h256, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+                DCX_CUDA(cudaStreamSynchronize(c.stream));
+            } else {
+                k_hist256<<<grid_for(in_bytes / 16 + 1, 256, 148 * 4), 256, 0, c.stream>>>(dsrc, in_bytes, c.d_h256);
+                DCX_CHECK_LAUNCH();
+                DCX_CUDA(cudaMemcpyAsync(h, c.d_h256, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+                DCX_CUDA(cudaStreamSynchronize(c.stream));
+            }
+        } else {
+            memset(h, 0, sizeof(h));
+        }
+        ByteMap map{};
+        uint32_t next = 1;
+        c.level0_entropy = 0;
+        for (int i = 0; i < 256; i++)
+            if (h[i]) {
+                map.m[i] = (uint8_t)(next++);
+                const double p = (double)h[i] / (double)std::max<uint64_t>(in_bytes, 1);
+                c.level0_entropy -= p * std::log2(p);
+            }
+        const uint64_t sigma = std::max<uint32_t>(next - 1, 1);
+        const bool wide = sigma == 256;
+        std::vector<uint64_t> in_off(offsets + s0, offsets + s1 + 1);
+        for (auto& v : in_off) v -= offsets[s0];
+        DBuf<uint64_t> d_inoff = upload(c, in_off);
+        DBuf<ByteMap> d_map(&c, 1);
+        DCX_CUDA(cudaMemcpyAsync(d_map.get(), &map, sizeof(map), cudaMemcpyHostToDevice, c.stream));
+        // small texts first (one launch), then the rest as segments of DCX levels
+        Segs small, big;
+        small.start = {0};
+        big.start = {0};
+        std::vector<uint32_t> small_ids, big_ids;
+        for (uint32_t s = s0; s < s1; s++) {
+            const uint64_t len = offsets[s + 1] - offsets[s];
+            if (len <= (uint64_t)std::min<uint32_t>(c.opt.small_threshold, SMALL_MAX)) {
+                small.start.push_back(small.start.back() + len + 1);
+                small_ids.push_back(s - s0);
+            } else {
+                big.start.push_back(big.start.back() + len + 1);
+                big_ids.push_back(s - s0);
+            }
+        }
+        // round output: the caller's device buffer, or a staging buffer copied back once
+        DBuf<uint8_t> rstage;
+        uint8_t* rout = (uint8_t*)sa_out + (offsets[s0] - base0) * wb;
+        if (!dev) {
+            rstage = DBuf<uint8_t>(&c, std::max<uint64_t>(in_bytes, 1) * wb + 16);
+            rout = rstage.get();
+        }
+        auto run_group = [&](const Segs& g, const std::vector<uint32_t>& ids) {
+            if (ids.empty()) return;
+            const uint32_t Kg = g.K();
+            std::vector<uint64_t> goff(Kg + 1, 0), gsrc(Kg);
+            for (uint32_t k = 0; k < Kg; k++) {
+                gsrc[k] = in_off[ids[k]];
+                goff[k + 1] = goff[k] + (in_off[ids[k] + 1] - in_off[ids[k]]);
+            }
+            DBuf<uint64_t> d_goff = upload(c, goff), d_gsrc = upload(c, gsrc);
+            const uint64_t Ng = g.N();
+            DBuf<uint8_t> gout(&c, std::max<uint64_t>(goff[Kg], 1) * wb + 16);
+            const uint32_t blocks = std::min<uint32_t>(Kg, 65535);
+            if (wide) {
+                DBuf<uint32_t> buf(&c, Ng + 1);
+                k_spread_texts<uint32_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), Kg, buf.get(),
+                                                                       d_map.get(), true);
+                DCX_CHECK_LAUNCH();
+                level<uint32_t>(c, buf.get(), g, sigma, X, 0, packing, gout.get(), width);
+            } else {
+                DBuf<uint8_t> buf(&c, Ng + 16);
+                k_spread_texts<uint8_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), Kg, buf.get(),
+                                                                      d_map.get(), false);
+                DCX_CHECK_LAUNCH();
+                level<uint8_t>(c, buf.get(), g, sigma, X, 0, packing, gout.get(), width);
+            }
+            k_scatter_outputs<<<blocks, 256, 0, c.stream>>>(gout.get(), d_gsrc.get(), d_goff.get(), Kg, rout,
+                                                           (uint32_t)wb);
+            DCX_CHECK_LAUNCH();
+            c.launched(2);
+        };
+        run_group(small, small_ids);
+        run_group(big, big_ids);
+        if (!dev && in_bytes)
+            DCX_CUDA(cudaMemcpyAsync((uint8_t*)sa_out + (offsets[s0] - base0) * wb, rout, in_bytes * wb,
+                                     cudaMemcpyDeviceToHost, c.stream));
+        DCX_CUDA(cudaStreamSynchronize(c.stream));
+        s0 = s1;
+    }
+    cudaEventRecord(e1, c.stream);
+    DCX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    c.st.ms_total = ms;
+    c.st.peak_bytes = c.peak;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+// Checks that sa (n entries of `width` bits) is the suffix array of text.
+static bool check_one(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, int width, uint32_t flags) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (n == 0) return true;
+    if (!text || !sa) throw Error(DCX_ERR_ARG, "null pointer");
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    const size_t wb = width / 8;
+    DBuf<uint8_t> t_in, sa_in;
+    const uint8_t* dtext = text;
+    const void* dsa = sa;
+    if (!dev) {
+        t_in = DBuf<uint8_t>(&c, n);
+        sa_in = DBuf<uint8_t>(&c, n * wb);
+        DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyHostToDevice, c.stream));
+        DCX_CUDA(cudaMemcpyAsync(sa_in.get(), sa, n * wb, cudaMemcpyHostToDevice, c.stream));
+        dtext = t_in.get();
+        dsa = sa_in.get();
+    }
+    DBuf<uint32_t> isa(&c, n);
+    DBuf<unsigned long long> bad(&c, 1);
+    DCX_CUDA(cudaMemsetAsync(isa.get(), 0, n * 4, c.stream));
+    DCX_CUDA(cudaMemsetAsync(bad.get(), 0, 8, c.stream));
+    k_check_isa<<<grid_for(n, 256), 256, 0, c.stream>>>(dsa, width, n, isa.get(), bad.get());
+    k_check_order<<<grid_for(n, 256), 256, 0, c.stream>>>(dsa, width, n, dtext, isa.get(), bad.get());
+    DCX_CHECK_LAUNCH();
+    return d2h_scalar(c, bad.get()) == 0;
 }
 
 }  // namespace dcx
@@ -1212,6 +1497,7 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
     } else if (s == "prefix_chars") o.prefix_chars = (uint32_t)value;
     else if (s == "trace") o.trace = value != 0;
     else if (s == "spin_limit") o.spin_limit = (uint32_t)value;
+    else if (s == "batch_round_cap") o.batch_round_cap = (uint64_t)value;
     else return DCX_ERR_ARG;
     return DCX_OK;
 }
@@ -1232,6 +1518,16 @@ int dcx_build_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, voi
 
 int dcx_build_sa_strict(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags) {
     return build_entry(x, text, n, dc, w, out, flags, true);
+}
+
+int dcx_check_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, int sa_width, uint32_t flags,
+                 int* ok) {
+    if (!x || !ok) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        *ok = dcx::check_one(x->c, text, n, sa, sa_width, flags) ? 1 : 0;
+    });
 }
 
 int dcx_get_stream(dcx_ctx* x, void** out) {
@@ -1258,8 +1554,14 @@ int dcx_get_trace(dcx_ctx* x, uint64_t* m_out, uint32_t* names, uint8_t* unique,
     return DCX_OK;
 }
 
-int dcx_build_sa_batch(dcx_ctx*, const uint8_t*, const uint64_t*, uint32_t, int, int, void*, uint32_t) {
-    return DCX_ERR_INTERNAL;
+int dcx_build_sa_batch(dcx_ctx* x, const uint8_t* texts, const uint64_t* offsets, uint32_t num_texts,
+                       int dc_or_auto, int sa_width, void* sa_out, uint32_t flags) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::build_batch(x->c, texts, offsets, num_texts, dc_or_auto, sa_width, sa_out, flags);
+    });
 }
 int dcx_serve_submit(dcx_ctx*, const uint8_t*, uint64_t, int, int, uint64_t*) { return DCX_ERR_INTERNAL; }
 int dcx_serve_poll(dcx_ctx*, uint64_t, void*, int*, double*) { return DCX_ERR_INTERNAL; }

@@ -37,9 +37,9 @@ __device__ __forceinline__ uint32_t ldc(const CharT* p) {
     return (uint32_t)__ldg(p);
 }
 
-// Encodes chars text[pos+off .. pos+off+plan.chars) (0 at or past n) into acc[0..KW).
+// Encodes chars text[start .. start+plan.chars) (0 at or past `end`) into acc[0..KW).
 template <int KW, typename CharT>
-__device__ __forceinline__ void encode_window(const CharT* text, uint64_t n, uint64_t start,
+__device__ __forceinline__ void encode_window(const CharT* text, uint64_t end, uint64_t start,
                                               const KeyPlan& plan, uint32_t* acc) {
 #pragma unroll
     for (int w = 0; w < KW; w++) acc[w] = 0;
@@ -49,7 +49,7 @@ __device__ __forceinline__ void encode_window(const CharT* text, uint64_t n, uin
         const uint32_t base = plan.base;
         uint32_t digit = 0;  // the chunk's chars in base sigma+1 (< chunk_mul[c] <= 2^32-1)
         for (uint32_t j = 0; j < len; j++, p++) {
-            uint32_t ch = p < n ? ldc(text + p) : 0u;
+            uint32_t ch = p < end ? ldc(text + p) : 0u;
             digit = digit * base + ch;
         }
         const uint32_t mul = plan.chunk_mul[c];
@@ -97,91 +97,138 @@ __device__ __forceinline__ void hist_flush(const uint32_t* sh, uint32_t bins, ui
     }
 }
 
-// Level keys: for every position i in [0, N) (N = n + 1: position n is the empty
-// suffix / dummy sample, key 0), key = window [i, i+chars), value = i.
-template <int KW, typename CharT>
-__global__ __launch_bounds__(256) void k_keys_prefix(const CharT* __restrict__ text, uint64_t n, uint64_t N,
+// Segments: a level holds K texts back to back, text s at [start[s], start[s+1]-1)
+// followed by one 0 at start[s+1]-1 (its empty suffix).  A window reads 0 from
+// its own text's end on, so windows never see the next text.  With K = 1 this
+// is the single text of length n = start[1] - 1.
+struct SegView {
+    uint32_t K;
+    const uint64_t* start;  // [K + 1]
+};
+
+__device__ __forceinline__ uint32_t seg_of(const SegView& sv, uint64_t p) {
+    uint32_t lo = 0, hi = sv.K;  // largest s with start[s] <= p
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sv.start[mid] <= p) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint64_t seg_end(const SegView& sv, uint32_t s) { return sv.start[s + 1] - 1; }
+
+// Level keys: for every position i in [0, N), key = window [i, i+chars) of i's
+// text, value = i; with K > 1 the text id is one more, most significant, word.
+template <int KW, bool SEG, typename CharT>
+__global__ __launch_bounds__(256) void k_keys_prefix(const CharT* __restrict__ text, uint64_t N, SegView sv,
                                                      KeyPlan plan, KeyOut ko, uint32_t* __restrict__ vals_out,
                                                      uint32_t* hist) {
-    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*KW * RADIX
-    hist_zero(sh, 4 * KW * RADIX);
+    constexpr int W = KW + (SEG ? 1 : 0);
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*W * RADIX
+    hist_zero(sh, 4 * W * RADIX);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t key[KW];
-        encode_window<KW>(text, n, i, plan, key);
+        const uint32_t sg = SEG ? seg_of(sv, i) : 0u;
+        uint32_t key[W];
+        encode_window<KW>(text, seg_end(sv, sg), i, plan, key);
+        if (SEG) key[W - 1] = sg;
 #pragma unroll
-        for (int w = 0; w < KW; w++) ko.w[w][i] = key[w];
+        for (int w = 0; w < W; w++) ko.w[w][i] = key[w];
         vals_out[i] = (uint32_t)i;
-        hist_add<KW>(sh, key);
+        hist_add<W>(sh, key);
     }
-    hist_flush(sh, 4 * KW * RADIX, hist);
+    hist_flush(sh, 4 * W * RADIX, hist);
 }
 
-// Level keys for windows that fit 64 bits, built with a sliding window: a CTA
+// Level keys for windows of at most 64 bits, built with a sliding window: a CTA
 // stages SLIDE_TILE + chars of text in shared memory, thread t encodes the
 // SLIDE_R consecutive positions [t*R, t*R + R) of the tile (one full encode,
-// then key' = (key - c_i * B^(P-1)) * B + c_{i+P} per step), and the keys are
-// written back through shared memory so global stores stay coalesced.  Chars
-// past the end of the text read as 0 (the padding char).
+// then key' = (key - c_i * B^(P-1)) * B + c_{i+P} per step, restarting at the
+// first position of each text), and the keys are written back through shared
+// memory so global stores stay coalesced.
 constexpr int SLIDE_THREADS = 256;
 constexpr int SLIDE_R = 16;
 constexpr int SLIDE_TILE = SLIDE_THREADS * SLIDE_R;
 constexpr int SLIDE_MAX_CHARS = 64;
 
-template <typename CharT>
-__global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __restrict__ text, uint64_t n, uint64_t N,
+template <bool SEG, typename CharT>
+__global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __restrict__ text, uint64_t N, SegView sv,
                                                               KeyPlan plan, uint64_t pow_top, KeyOut ko,
                                                               uint32_t* __restrict__ vals_out, uint32_t* hist) {
-    extern __shared__ uint32_t sh[];  // HIST_COPIES * 8 * RADIX histogram words, then the staging area
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 12 * RADIX histogram words, then the staging area
     uint32_t* hst = sh;
-    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 8 * RADIX);  // SLIDE_TILE keys
-    CharT* s_chars = reinterpret_cast<CharT*>(s_keys + SLIDE_TILE);             // SLIDE_TILE + P chars
-    hist_zero(hst, 8 * RADIX);
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 12 * RADIX);  // SLIDE_TILE keys
+    uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_keys + SLIDE_TILE);             // SLIDE_TILE text ids
+    CharT* s_chars = reinterpret_cast<CharT*>(s_seg + SLIDE_TILE);                  // SLIDE_TILE + P chars
+    const uint32_t W = plan.kw + (SEG ? 1 : 0);
+    hist_zero(hst, 4 * W * RADIX);
     const uint32_t P = plan.chars;
     const uint64_t B = plan.base;
     for (uint64_t base = (uint64_t)blockIdx.x * SLIDE_TILE; base < N; base += (uint64_t)gridDim.x * SLIDE_TILE) {
         for (uint32_t i = threadIdx.x; i < SLIDE_TILE + P; i += SLIDE_THREADS) {
             const uint64_t p = base + i;
-            s_chars[i] = p < n ? text[p] : CharT(0);
+            s_chars[i] = p < N ? text[p] : CharT(0);
         }
         __syncthreads();
         const uint32_t r0 = threadIdx.x * SLIDE_R;
-        uint64_t key = 0;
-        for (uint32_t j = 0; j < P; j++) key = key * B + (uint32_t)s_chars[r0 + j];
+        uint32_t sg = SEG ? seg_of(sv, base + r0) : 0u;
+        uint64_t end = seg_end(sv, sg);  // position of the text's 0
+        auto full = [&](uint32_t r) {     // window of tile position r, cut at `end`
+            uint64_t k = 0;
+            for (uint32_t j = 0; j < P; j++) k = k * B + ((base + r + j < end) ? (uint32_t)s_chars[r + j] : 0u);
+            return k;
+        };
+        uint64_t key = full(r0);
 #pragma unroll
         for (int r = 0; r < SLIDE_R; r++) {
+            const uint64_t i = base + r0 + r;
             s_keys[r0 + r] = key;
-            const uint32_t out = (uint32_t)s_chars[r0 + r];
-            key = (key - (uint64_t)out * pow_top) * B + (uint32_t)s_chars[r0 + r + P];
+            if (SEG) s_seg[r0 + r] = sg;
+            if (i == end) {  // next position starts the next text
+                if (SEG && sg + 1 < sv.K) {
+                    sg++;
+                    end = seg_end(sv, sg);
+                }
+                key = full(r0 + r + 1);
+            } else {
+                const uint32_t out = (uint32_t)s_chars[r0 + r];
+                const uint32_t in = (i + P < end) ? (uint32_t)s_chars[r0 + r + P] : 0u;
+                key = (key - (uint64_t)out * pow_top) * B + in;
+            }
         }
         __syncthreads();
         const uint32_t tile_n = (uint32_t)((N - base) < SLIDE_TILE ? (N - base) : SLIDE_TILE);
         for (uint32_t i = threadIdx.x; i < tile_n; i += SLIDE_THREADS) {
             const uint64_t k = s_keys[i];
-            uint32_t kk[2] = {(uint32_t)k, (uint32_t)(k >> 32)};
+            uint32_t kk[3] = {(uint32_t)k, (uint32_t)(k >> 32), 0u};
             ko.w[0][base + i] = kk[0];
             if (plan.kw > 1) ko.w[1][base + i] = kk[1];
+            if (SEG) {
+                kk[plan.kw] = s_seg[i];
+                ko.w[plan.kw][base + i] = s_seg[i];
+            }
             vals_out[base + i] = (uint32_t)(base + i);
-            if (plan.kw > 1) hist_add<2>(hst, kk);
+            if (W == 3) hist_add<3>(hst, kk);
+            else if (W == 2) hist_add<2>(hst, kk);
             else hist_add<1>(hst, kk);
         }
         __syncthreads();
     }
-    hist_flush(hst, 4 * plan.kw * RADIX, hist);
+    hist_flush(hst, 4 * W * RADIX, hist);
 }
 
 template <typename CharT>
 constexpr size_t keys_slide_smem() {
-    return sizeof(uint32_t) * HIST_COPIES * 8 * RADIX + sizeof(uint64_t) * SLIDE_TILE +
+    return sizeof(uint32_t) * HIST_COPIES * 12 * RADIX + sizeof(uint64_t) * SLIDE_TILE + sizeof(uint32_t) * SLIDE_TILE +
            sizeof(CharT) * (SLIDE_TILE + SLIDE_MAX_CHARS);
 }
 
 // Refinement keys for the elements of tie groups: element j has text position
-// tpos[j] and group number grp[j].  The key is
-// (group number in the top word, window [pos+off, pos+off+chars) below it);
-// value = text position.
+// tpos[j], text tseg[j] and group number grp[j].  The key is (group number in
+// the top word, window [pos+off, pos+off+chars) of its text below it); value =
+// text position.
 template <int KW, typename CharT>
-__global__ __launch_bounds__(256) void k_keys_refine(const CharT* __restrict__ text, uint64_t n, uint64_t count,
+__global__ __launch_bounds__(256) void k_keys_refine(const CharT* __restrict__ text, SegView sv, uint64_t count,
                                                      const uint32_t* __restrict__ tpos,
+                                                     const uint32_t* __restrict__ tseg,
                                                      const uint32_t* __restrict__ grp, uint32_t off,
                                                      KeyPlan plan, KeyOut ko, uint32_t* __restrict__ vals_out,
                                                      uint32_t* hist) {
@@ -190,8 +237,9 @@ __global__ __launch_bounds__(256) void k_keys_refine(const CharT* __restrict__ t
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < count;
          j += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t pos = tpos[j];
+        const uint64_t end = seg_end(sv, tseg ? tseg[j] : 0u);
         uint32_t key[KW + 1];
-        encode_window<KW>(text, n, (uint64_t)pos + off, plan, key);
+        encode_window<KW>(text, end, (uint64_t)pos + off, plan, key);
         key[KW] = grp[j];
 #pragma unroll
         for (int w = 0; w <= KW; w++) ko.w[w][j] = key[w];

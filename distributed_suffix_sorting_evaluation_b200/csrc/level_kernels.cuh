@@ -1,6 +1,13 @@
 // Per-level kernels of the DCX pipeline other than the sorts: alphabet remap,
 // head flags, the scan operators of naming / compaction / group detection, the
-// recursion string in (mod X, div X) order with discarding, and SA emission.
+// recursion string in (mod X, div X) order with discarding, SA emission and the
+// suffix-array checker.
+//
+// A level holds K >= 1 texts back to back (text s occupies [start[s],
+// start[s+1]-1) and is followed by one 0 which is its empty suffix).  Every
+// position-dependent rule of the reference -- which positions are samples, the
+// dummy sample, samples_before, the rank slot (i/X)*D + NEXT_RANK[i%X] -- is
+// applied per text with local positions; K = 1 is the single-text build.
 #pragma once
 
 #include "common.cuh"
@@ -13,11 +20,35 @@ struct DcFlags {
     uint8_t in_dc[MAX_X];
     uint32_t next_rank[MAX_X];
     uint32_t dc[MAX_D];
-    uint64_t samples_before[MAX_D + 1];
 };
 
-__device__ __forceinline__ uint64_t rank_pos_of(uint32_t pos, const DcFlags& f) {
-    return (uint64_t)(pos / f.X) * f.D + f.next_rank[pos % f.X];
+// Recursion modes per text.
+enum : uint8_t { REC_NONE = 0, REC_DIRECT = 1, REC_DISCARD = 2 };
+
+// Per-level segment tables (device arrays).
+struct LevelSeg {
+    uint32_t K;
+    const uint64_t* start;  // [K+1] first position of text s; start[K] = N
+    const uint64_t* rbase;  // [K+1] first sample slot of text s (texts are padded by D zero slots)
+    const uint64_t* qbase;  // [K+1] first position of text s in the (mod X, div X) string
+    const uint64_t* sb;     // [K*(D+1)] samples_before of text s (pdcx.hpp:503-508)
+    const uint64_t* obase;  // [K+1] first output slot of text s (sum of text lengths)
+    const uint8_t* mode;    // [K] recursion mode
+    const uint64_t* kbase;  // [K+1] first kept index of text s (scan of keep flags)
+    const uint64_t* start2; // [K] first position of text s in the recursion input
+};
+
+__device__ __forceinline__ uint32_t bsearch_le(const uint64_t* a, uint32_t K, uint64_t v) {
+    uint32_t lo = 0, hi = K;  // largest s < K with a[s] <= v
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] <= v) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t slot_of_local(uint64_t i, const DcFlags& f) {
+    return (i / f.X) * f.D + f.next_rank[i % f.X];
 }
 
 // ---- alphabet (cli.cpp:417-463) ---------------------------------------------
@@ -71,9 +102,44 @@ __global__ void k_remap(const uint8_t* __restrict__ in, uint8_t* __restrict__ ou
         out[i] = m[in[i]];
 }
 
+// byte b -> b + 1 in 32-bit chars (all 256 byte values present)
 __global__ void k_widen_text(const uint8_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ out) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         out[i] = (uint32_t)in[i] + 1u;
+}
+
+// Batch layout: text k of a group (src_off[k] in the round input, length
+// goff[k+1] - goff[k]) moves to goff[k] + k of the level buffer, leaving one 0
+// after every text.  A thread block per text; `widen` maps byte b to the
+// 32-bit char b + 1, otherwise the round's alphabet map applies.
+template <typename CharT>
+__global__ void k_spread_texts(const uint8_t* __restrict__ in, const uint64_t* __restrict__ src_off,
+                               const uint64_t* __restrict__ goff, uint32_t K, CharT* __restrict__ out,
+                               const ByteMap* __restrict__ map, bool widen) {
+    __shared__ uint8_t m[256];
+    if (!widen)
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) m[i] = map->m[i];
+    __syncthreads();
+    for (uint32_t k = blockIdx.x; k < K; k += gridDim.x) {
+        const uint64_t len = goff[k + 1] - goff[k];
+        const uint8_t* src = in + src_off[k];
+        CharT* o = out + goff[k] + k;
+        for (uint64_t i = threadIdx.x; i < len; i += blockDim.x)
+            o[i] = widen ? (CharT)((uint32_t)src[i] + 1u) : (CharT)m[src[i]];
+        if (threadIdx.x == 0) o[len] = CharT(0);
+    }
+}
+
+// Group outputs (goff layout, wb bytes per entry) to the texts' slots in the
+// round's output (src_off layout).
+__global__ void k_scatter_outputs(const uint8_t* __restrict__ gout, const uint64_t* __restrict__ src_off,
+                                  const uint64_t* __restrict__ goff, uint32_t K, uint8_t* __restrict__ out, uint32_t wb) {
+    for (uint32_t k = blockIdx.x; k < K; k += gridDim.x) {
+        const uint64_t bytes = (goff[k + 1] - goff[k]) * wb;
+        const uint8_t* src = gout + goff[k] * wb;
+        uint8_t* dst = out + src_off[k] * wb;
+        for (uint64_t i = threadIdx.x; i < bytes; i += blockDim.x) dst[i] = src[i];
+    }
 }
 
 // ---- head flags --------------------------------------------------------------
@@ -95,14 +161,16 @@ __global__ void k_heads(KeyWords k, uint32_t kw, uint64_t N, uint8_t* __restrict
 // ---- scan operators (two 32-bit counters packed in a uint64) ------------------
 // Tie groups of a partially sorted array: element k is tied when its group
 // (run between head flags) has two or more elements.  Emits the tied elements'
-// slots and dense group numbers.
+// slots, dense group numbers, positions and texts.
 struct OpTied {
     const uint8_t* head;
     uint64_t N;
     const uint32_t* sa;
+    const uint32_t* segw;  // text of each sorted element, or null for one text
     uint32_t* slot;
     uint32_t* grp;
     uint32_t* tpos;
+    uint32_t* tseg;
     __device__ uint64_t load(uint64_t k) const {
         const uint32_t h = head[k];
         const uint32_t nh = (k + 1 < N) ? head[k + 1] : 1u;
@@ -115,6 +183,7 @@ struct OpTied {
             slot[j] = (uint32_t)k;
             grp[j] = (uint32_t)ex + (uint32_t)v;  // inclusive group number
             tpos[j] = sa[k];
+            if (tseg) tseg[j] = segw[k];
         }
     }
 };
@@ -135,25 +204,33 @@ __global__ void k_refine_scatter(uint64_t count, const uint32_t* __restrict__ sl
     }
 }
 
-// Phase 2 step 1: samples in sorted order with the group number of their window
-// (compute_lexicographic_ranks, compute_ranks.hpp:89-111).
+// Phase 2 step 1: samples in window order with the group number of their window
+// (compute_lexicographic_ranks, compute_ranks.hpp:89-111).  A position is a
+// sample when its local index mod X is in the cover; the text's empty suffix
+// (local index n_s) is then the dummy sample of pdcx.hpp:482-501.
 struct OpSamples {
     const uint8_t* head;
     const uint32_t* sa;
+    const uint32_t* segw;
     const DcFlags* f;
-    uint32_t* s_pos;
+    LevelSeg ls;
+    uint32_t* s_pos;  // local index
+    uint32_t* s_seg;
     uint32_t* s_grp;
     uint64_t cap;
     __device__ uint64_t load(uint64_t k) const {
-        const uint32_t pos = sa[k];
-        const uint32_t smp = f->in_dc[pos % f->X];
+        const uint32_t sg = segw ? segw[k] : 0u;
+        const uint64_t i = sa[k] - ls.start[sg];
+        const uint32_t smp = f->in_dc[i % f->X];
         return (uint64_t)head[k] | ((uint64_t)smp << 32);
     }
     __device__ void store(uint64_t k, uint64_t ex, uint64_t v) const {
         if (v >> 32) {
             const uint32_t j = (uint32_t)(ex >> 32);
             if (j >= cap) return;
-            s_pos[j] = sa[k];
+            const uint32_t sg = segw ? segw[k] : 0u;
+            s_pos[j] = (uint32_t)(sa[k] - ls.start[sg]);
+            s_seg[j] = sg;
             s_grp[j] = (uint32_t)ex + (uint32_t)v;
         }
     }
@@ -174,29 +251,32 @@ struct OpNames {
     }
 };
 
-// Sample records in sample text order (slot k = (p/X)*D + NEXT_RANK[p%X] of
-// sample p): bits [0,32) name, bit 32 unique flag, bits [33,64) index j of the
-// sample in window order.  One random 8-byte write per sample; every later step
-// of phase 3 reads these records with coalesced passes.
+// Sample records in sample text order (slot rbase[s] + (i/X)*D + NEXT_RANK[i%X]
+// of sample i of text s): bits [0,32) name, bit 32 unique flag, bits [33,64)
+// index j of the sample in window order.  The D padding slots after each text
+// keep the all-ones pattern (SREC_EMPTY).  One random 8-byte write per sample;
+// every later step of phase 3 reads these records with coalesced passes.
+constexpr uint64_t SREC_EMPTY = ~0ull;
 __device__ __forceinline__ uint32_t srec_name(uint64_t r) { return (uint32_t)r; }
 __device__ __forceinline__ uint32_t srec_uniq(uint64_t r) { return (uint32_t)(r >> 32) & 1u; }
 __device__ __forceinline__ uint32_t srec_j(uint64_t r) { return (uint32_t)(r >> 33); }
 
-__global__ void k_scatter_samples(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ name,
-                                  const uint8_t* __restrict__ uniq, const DcFlags* __restrict__ f,
-                                  uint64_t* __restrict__ srec) {
+__global__ void k_scatter_samples(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ s_seg,
+                                  const uint32_t* __restrict__ name, const uint8_t* __restrict__ uniq,
+                                  const DcFlags* __restrict__ f, LevelSeg ls, uint64_t* __restrict__ srec) {
     const DcFlags& F = *f;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = rank_pos_of(s_pos[j], F);
+        const uint64_t k = ls.rbase[s_seg[j]] + slot_of_local(s_pos[j], F);
         srec[k] = (uint64_t)name[j] | ((uint64_t)uniq[j] << 32) | ((uint64_t)j << 33);
     }
 }
 
-// Distinct names: the rank of every sample is its name.
-__global__ void k_ranks_from_names(uint64_t m, const uint64_t* __restrict__ srec, uint32_t* __restrict__ rank_text,
+// Distinct names: the rank of every sample is its name (padding slots stay 0).
+__global__ void k_ranks_from_names(uint64_t slots, const uint64_t* __restrict__ srec, uint32_t* __restrict__ rank_text,
                                    uint32_t* trace_names, uint8_t* trace_uniq) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < slots; k += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t r = srec[k];
+        if (r == SREC_EMPTY) continue;
         if (rank_text) rank_text[k] = srec_name(r);
         if (trace_names) {
             trace_names[k] = srec_name(r);
@@ -205,50 +285,130 @@ __global__ void k_ranks_from_names(uint64_t m, const uint64_t* __restrict__ srec
     }
 }
 
-// Recursion string in (mod X, div X) order: position q = samples_before[c] + b
-// holds the name of sample slot k = b*D + c (a transpose of the D-column layout).
-__global__ void k_rec_from_samples(uint64_t m, const uint64_t* __restrict__ srec, const DcFlags* __restrict__ f,
-                                   uint32_t* __restrict__ rec, uint8_t* __restrict__ rec_uniq) {
-    const DcFlags& F = *f;
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t c = 0;
-        while (c + 1 < F.D && q >= F.samples_before[c + 1]) c++;
-        const uint64_t b = q - F.samples_before[c];
-        const uint64_t r = srec[b * F.D + c];
+// Recursion string in (mod X, div X) order per text (DCRankIndex::cmp_mod_div,
+// compute_ranks.hpp:49-56): position qbase[s] + samples_before_s[c] + b holds
+// the name of the text's sample slot b*D + c.  rec_flag bit 0 = unique, bit 1 =
+// first element of its text's string.
+__device__ __forceinline__ void q_to_slot(uint64_t q, const LevelSeg& ls, uint32_t D, uint32_t& s, uint64_t& slot) {
+    s = ls.K > 1 ? bsearch_le(ls.qbase, ls.K, q) : 0u;
+    const uint64_t ql = q - ls.qbase[s];
+    const uint64_t* sb = ls.sb + (uint64_t)s * (D + 1);
+    uint32_t c = 0;
+    while (c + 1 < D && ql >= sb[c + 1]) c++;
+    slot = ls.rbase[s] + (ql - sb[c]) * D + c;
+}
+
+__global__ void k_rec_from_samples(uint64_t Mq, const uint64_t* __restrict__ srec, const DcFlags* __restrict__ f,
+                                   LevelSeg ls, uint32_t* __restrict__ rec, uint8_t* __restrict__ rec_flag) {
+    const uint32_t D = f->D;
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < Mq; q += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t s;
+        uint64_t slot;
+        q_to_slot(q, ls, D, s, slot);
+        const uint64_t r = srec[slot];
         rec[q] = srec_name(r);
-        rec_uniq[q] = (uint8_t)srec_uniq(r);
+        rec_flag[q] = (uint8_t)(srec_uniq(r) | ((q == ls.qbase[s]) ? 2u : 0u));
     }
 }
 
-// After discarding, unique samples keep their window order: rank = j + 1.
-__global__ void k_ranks_unique_text(uint64_t m, const uint64_t* __restrict__ srec, uint32_t* __restrict__ rank_text) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t r = srec[k];
-        if (srec_uniq(r)) rank_text[k] = srec_j(r) + 1;
+// Discarding rule (num_ranks_after_discarding, pdcx.hpp:215-228): keep q unless it
+// and its predecessor in the same text's string are both unique; the first
+// element of each text's string is always kept.
+__device__ __forceinline__ uint32_t discard_keep(const uint8_t* rec_flag, uint64_t q) {
+    const uint32_t fl = rec_flag[q];
+    if (fl & 2u) return 1u;
+    return !((fl & 1u) && (rec_flag[q - 1] & 1u));
+}
+
+// Counting pass: exclusive prefix of the discarding rule over all texts.
+struct OpKeepCount {
+    const uint8_t* rec_flag;
+    uint32_t* kidx;
+    __device__ uint32_t load(uint64_t q) const { return discard_keep(rec_flag, q); }
+    __device__ void store(uint64_t q, uint32_t ex, uint32_t) const { kidx[q] = ex; }
+};
+
+// Compaction into the recursion input: per text, nothing (names distinct), all
+// (direct recursion) or the discarding rule.  Text s's kept elements land at
+// start2[s] + (kept index - kbase[s]); separators stay 0 (buffer zeroed).
+struct OpCompact {
+    const uint8_t* rec_flag;
+    const uint32_t* rec;
+    LevelSeg ls;
+    uint32_t* rec2;
+    uint32_t* kidx;
+    __device__ uint32_t load(uint64_t q) const {
+        const uint32_t s = ls.K > 1 ? bsearch_le(ls.qbase, ls.K, q) : 0u;
+        const uint8_t md = ls.mode[s];
+        if (md == REC_NONE) return 0u;
+        if (md == REC_DIRECT) return 1u;
+        return discard_keep(rec_flag, q);
+    }
+    __device__ void store(uint64_t q, uint32_t ex, uint32_t v) const {
+        if (!v) return;
+        const uint32_t s = ls.K > 1 ? bsearch_le(ls.qbase, ls.K, q) : 0u;
+        rec2[ls.start2[s] + (ex - ls.kbase[s])] = rec[q];
+        kidx[q] = ex;
+    }
+};
+
+// Results of the recursive call.  sa2 holds, for each recursing text r (in
+// order), the suffix array of its reduced string at o2[r].  Direct texts: the
+// sample at string position q gets rank k + 1 (pdcx.hpp:183-212, map_back 83-94).
+// Discarding texts: rank_of[kept index] = k + 1 (pdcx.hpp:264-291).
+__global__ void k_after_recursion(uint64_t total2, const uint32_t* __restrict__ sa2, const uint64_t* __restrict__ o2,
+                                  uint32_t R, const uint32_t* __restrict__ rec_text, const DcFlags* __restrict__ f,
+                                  LevelSeg ls, uint32_t* __restrict__ rank_text, uint32_t* __restrict__ rank_of) {
+    const uint32_t D = f->D;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total2;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = R > 1 ? bsearch_le(o2, R, x) : 0u;
+        const uint32_t s = rec_text[r];
+        const uint64_t k = x - o2[r];
+        const uint64_t ql = sa2[x];
+        if (ls.mode[s] == REC_DIRECT) {
+            const uint64_t* sb = ls.sb + (uint64_t)s * (D + 1);
+            uint32_t c = 0;
+            while (c + 1 < D && ql >= sb[c + 1]) c++;
+            rank_text[ls.rbase[s] + (ql - sb[c]) * D + c] = (uint32_t)(k + 1);
+        } else {
+            rank_of[ls.kbase[s] + ql] = (uint32_t)(k + 1);
+        }
     }
 }
 
-// Non-unique samples (text order) keyed by (name, rank of their position in the
-// reduced string); value = sample slot k.
-struct OpNonUniqueText {
+// Non-unique samples of discarding texts keyed by (name, rank of their position
+// in the reduced string); value = sample slot (pdcx.hpp:296-346).
+struct OpNonUniqueSeg {
     const uint64_t* srec;
     const DcFlags* f;
+    LevelSeg ls;
     const uint32_t* kidx;
     const uint32_t* rank_of;
     uint32_t* key_lo;
     uint32_t* key_hi;
     uint32_t* val;
-    __device__ uint32_t load(uint64_t k) const { return !srec_uniq(srec[k]); }
+    __device__ uint32_t load(uint64_t k) const {
+        const uint64_t r = srec[k];
+        if (r == SREC_EMPTY || srec_uniq(r)) return 0u;
+        const uint32_t s = ls.K > 1 ? bsearch_le(ls.rbase, ls.K, k) : 0u;
+        return ls.mode[s] == REC_DISCARD;
+    }
     __device__ void store(uint64_t k, uint32_t ex, uint32_t v) const {
-        if (v && key_lo) {  // null outputs: counting pass only
-            const uint64_t b = k / f->D, c = k % f->D;
-            const uint64_t q = f->samples_before[c] + b;
-            key_lo[ex] = rank_of[kidx[q]];
-            key_hi[ex] = srec_name(srec[k]);
-            val[ex] = (uint32_t)k;
-        }
+        if (!v || !key_lo) return;  // null outputs: counting pass only
+        const uint32_t s = ls.K > 1 ? bsearch_le(ls.rbase, ls.K, k) : 0u;
+        const uint64_t kl = k - ls.rbase[s];
+        const uint64_t q = ls.qbase[s] + ls.sb[(uint64_t)s * (f->D + 1) + kl % f->D] + kl / f->D;
+        key_lo[ex] = rank_of[kidx[q]];
+        key_hi[ex] = srec_name(srec[k]);
+        val[ex] = (uint32_t)k;
     }
 };
+
+__global__ void k_name_starts(uint64_t m, const uint32_t* __restrict__ name, uint32_t* __restrict__ start_of) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x)
+        if (j == 0 || name[j] != name[j - 1]) start_of[name[j]] = (uint32_t)j;
+}
 
 __global__ void k_ranks_nonunique(uint64_t mu, const uint32_t* __restrict__ key_hi, const uint32_t* __restrict__ val,
                                   const uint32_t* __restrict__ start_s, const uint32_t* __restrict__ start_l,
@@ -259,154 +419,25 @@ __global__ void k_ranks_nonunique(uint64_t mu, const uint32_t* __restrict__ key_
     }
 }
 
-// Final SA of a level: sa_full slot 0 is position n (the empty suffix); the
-// n remaining slots are written in 32-, 40- (little endian, high byte 0 since
-// indices are < 2^32) or 64-bit form.  Four entries per thread so the 40-bit
-// form is written as five aligned 32-bit words.
-__global__ void k_emit(const uint32_t* __restrict__ sa_full, uint64_t n, void* __restrict__ out, int width) {
-    const uint64_t groups = n / 4;
-    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t e0 = sa_full[4 * g + 1], e1 = sa_full[4 * g + 2], e2 = sa_full[4 * g + 3], e3 = sa_full[4 * g + 4];
-        if (width == 32) {
-            reinterpret_cast<uint4*>(out)[g] = make_uint4(e0, e1, e2, e3);
-        } else if (width == 64) {
-            ulonglong2* o = reinterpret_cast<ulonglong2*>(out) + 2 * g;
-            o[0] = make_ulonglong2(e0, e1);
-            o[1] = make_ulonglong2(e2, e3);
-        } else {
-            uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * g;
-            o[0] = e0;
-            o[1] = e1 << 8;
-            o[2] = (e1 >> 24) | (e2 << 16);
-            o[3] = (e2 >> 16) | (e3 << 24);
-            o[4] = e3 >> 8;
-        }
-    }
-    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
-        const uint64_t k = groups * 4 + threadIdx.x;
-        const uint32_t v = sa_full[k + 1];
-        if (width == 32) reinterpret_cast<uint32_t*>(out)[k] = v;
-        else if (width == 64) reinterpret_cast<uint64_t*>(out)[k] = v;
-        else {
-            uint8_t* o = reinterpret_cast<uint8_t*>(out) + 5 * k;
-            o[0] = (uint8_t)v;
-            o[1] = (uint8_t)(v >> 8);
-            o[2] = (uint8_t)(v >> 16);
-            o[3] = (uint8_t)(v >> 24);
-            o[4] = 0;
-        }
+// Ranks that need no recursion result: texts with distinct names keep their
+// names; unique samples of discarding texts keep their window order (j + 1).
+__global__ void k_ranks_rest(uint64_t slots, const uint64_t* __restrict__ srec, LevelSeg ls,
+                             uint32_t* __restrict__ rank_text) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < slots; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = srec[k];
+        if (r == SREC_EMPTY) continue;
+        const uint32_t s = ls.K > 1 ? bsearch_le(ls.rbase, ls.K, k) : 0u;
+        const uint8_t md = ls.mode[s];
+        if (md == REC_NONE) rank_text[k] = srec_name(r);
+        else if (md == REC_DISCARD && srec_uniq(r)) rank_text[k] = srec_j(r) + 1;
     }
 }
 
-// Phase 3 distinct case: ranks = names, scattered to sample text order.
-__global__ void k_scatter_names(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ name,
-                                const DcFlags* __restrict__ f, uint32_t* __restrict__ rank_text,
-                                uint32_t* trace_names, uint8_t* trace_uniq, const uint8_t* uniq) {
-    const DcFlags& F = *f;
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t rp = rank_pos_of(s_pos[j], F);
-        if (rank_text) rank_text[rp] = name[j];
-        if (trace_names) {
-            trace_names[rp] = name[j];
-            trace_uniq[rp] = uniq[j];
-        }
-    }
-}
-
-// Recursion string in (mod X, div X) order (DCRankIndex::cmp_mod_div,
-// compute_ranks.hpp:49-56): sample p = b*X + DC[c] goes to samples_before[c] + b.
-__global__ void k_build_rec(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ name,
-                            const uint8_t* __restrict__ uniq, const DcFlags* __restrict__ f, uint32_t* __restrict__ rec,
-                            uint8_t* __restrict__ rec_uniq, uint32_t* __restrict__ q_of_j) {
-    const DcFlags& F = *f;
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t pos = s_pos[j];
-        const uint32_t c = F.next_rank[pos % F.X];
-        const uint64_t q = F.samples_before[c] + pos / F.X;
-        rec[q] = name[j];
-        rec_uniq[q] = uniq[j];
-        if (q_of_j) q_of_j[j] = (uint32_t)q;
-    }
-}
-
-// Direct recursion result: sample at recursion index SA_R[k] has rank k+1
-// (recursive_call_direct + map_back, pdcx.hpp:83-94,183-212).
-__global__ void k_ranks_from_rec(uint64_t m, const uint32_t* __restrict__ sa_r, const DcFlags* __restrict__ f,
-                                 uint32_t* __restrict__ rank_text) {
-    const DcFlags& F = *f;
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t q = sa_r[k];
-        uint32_t c = 0;
-        while (c + 1 < F.D && q >= F.samples_before[c + 1]) c++;
-        const uint64_t b = q - F.samples_before[c];
-        rank_text[b * F.D + c] = (uint32_t)(k + 1);
-    }
-}
-
-// Discarding (num_ranks_after_discarding / recursive_call_with_discarding,
-// pdcx.hpp:215-252): keep element q unless it and its predecessor are unique.
-struct OpKeep {
-    const uint8_t* rec_uniq;
-    const uint32_t* rec;
-    uint32_t* rec2;
-    uint32_t* kidx;
-    __device__ uint32_t load(uint64_t q) const { return q == 0 || !(rec_uniq[q] && rec_uniq[q - 1]); }
-    __device__ void store(uint64_t q, uint32_t ex, uint32_t v) const {
-        if (rec2 && v) rec2[ex] = rec[q];
-        if (kidx) kidx[q] = ex;
-    }
-};
-
-__global__ void k_inverse(uint64_t m, const uint32_t* __restrict__ sa, uint32_t* __restrict__ inv) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x)
-        inv[sa[k]] = (uint32_t)(k + 1);
-}
-
-// Non-unique samples with (name, rank2) keys for the rank recovery after
-// discarding (pdcx.hpp:296-346).  rank2 = rank of the sample's position in the
-// reduced string.
-struct OpNonUnique {
-    const uint8_t* uniq;
-    const uint32_t* name;
-    const uint32_t* q_of_j;
-    const uint32_t* kidx;
-    const uint32_t* rank_of;
-    uint32_t* key_lo;
-    uint32_t* key_hi;
-    uint32_t* val;
-    __device__ uint32_t load(uint64_t j) const { return !uniq[j]; }
-    __device__ void store(uint64_t j, uint32_t ex, uint32_t v) const {
-        if (v) {
-            key_lo[ex] = rank_of[kidx[q_of_j[j]]];
-            key_hi[ex] = name[j];
-            val[ex] = (uint32_t)j;
-        }
-    }
-};
-
-__global__ void k_name_starts(uint64_t m, const uint32_t* __restrict__ name, uint32_t* __restrict__ start_of) {
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x)
-        if (j == 0 || name[j] != name[j - 1]) start_of[name[j]] = (uint32_t)j;
-}
-
-__global__ void k_ranks_after_discarding(uint64_t mu, const uint32_t* __restrict__ key_hi,
-                                         const uint32_t* __restrict__ val, const uint32_t* __restrict__ start_s,
-                                         const uint32_t* __restrict__ start_l, const uint32_t* __restrict__ s_pos,
-                                         const DcFlags* __restrict__ f, uint32_t* __restrict__ rank_text) {
-    const DcFlags& F = *f;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < mu; t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t nm = key_hi[t];
-        const uint32_t j = val[t];
-        const uint32_t r = start_s[nm] + (uint32_t)(t - start_l[nm]) + 1;
-        rank_text[rank_pos_of(s_pos[j], F)] = r;
-    }
-}
-
-__global__ void k_ranks_unique(uint64_t m, const uint8_t* __restrict__ uniq, const uint32_t* __restrict__ s_pos,
-                               const DcFlags* __restrict__ f, uint32_t* __restrict__ rank_text) {
-    const DcFlags& F = *f;
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x)
-        if (uniq[j]) rank_text[rank_pos_of(s_pos[j], F)] = (uint32_t)(j + 1);
+// out[i] = src[idx[i]] (idx[i] == total_idx reads total_val instead)
+__global__ void k_gather_u32(const uint32_t* __restrict__ src, const uint64_t* __restrict__ idx, uint32_t count,
+                             uint64_t total_idx, uint32_t total_val, uint32_t* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        out[i] = idx[i] < total_idx ? src[idx[i]] : total_val;
 }
 
 // ---- phase 4 tie groups --------------------------------------------------------
@@ -499,25 +530,114 @@ __global__ void k_copy_ranges(const uint64_t* __restrict__ offsets, uint32_t ngr
 }
 
 // ---- SA emission --------------------------------------------------------------
-// sa_full holds N = n + 1 slots; slot 0 is position n (the empty suffix).
-__global__ void k_emit32(const uint32_t* __restrict__ sa_full, uint64_t n, uint32_t* __restrict__ out) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
-        out[k] = sa_full[k + 1];
-}
-
-__global__ void k_widen(const uint32_t* __restrict__ sa, uint64_t n, uint8_t* __restrict__ out, int width) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t v = sa[k];
-        if (width == 64) {
-            reinterpret_cast<uint64_t*>(out)[k] = v;
-        } else {  // 40-bit little endian: low uint32 then high uint8 (util/uint_types.hpp:49-269)
-            uint8_t* o = out + 5 * k;
+// One text: sa_full slot 0 is position n (the empty suffix); the n remaining
+// slots are written in 32-, 40- (little endian, high byte 0 since indices are
+// < 2^32) or 64-bit form.  Four entries per thread so the 40-bit form is
+// written as five aligned 32-bit words.
+__global__ void k_emit(const uint32_t* __restrict__ sa_full, uint64_t n, void* __restrict__ out, int width) {
+    const uint64_t groups = n / 4;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t e0 = sa_full[4 * g + 1], e1 = sa_full[4 * g + 2], e2 = sa_full[4 * g + 3], e3 = sa_full[4 * g + 4];
+        if (width == 32) {
+            reinterpret_cast<uint4*>(out)[g] = make_uint4(e0, e1, e2, e3);
+        } else if (width == 64) {
+            ulonglong2* o = reinterpret_cast<ulonglong2*>(out) + 2 * g;
+            o[0] = make_ulonglong2(e0, e1);
+            o[1] = make_ulonglong2(e2, e3);
+        } else {
+            uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * g;
+            o[0] = e0;
+            o[1] = e1 << 8;
+            o[2] = (e1 >> 24) | (e2 << 16);
+            o[3] = (e2 >> 16) | (e3 << 24);
+            o[4] = e3 >> 8;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+        const uint64_t k = groups * 4 + threadIdx.x;
+        const uint32_t v = sa_full[k + 1];
+        if (width == 32) reinterpret_cast<uint32_t*>(out)[k] = v;
+        else if (width == 64) reinterpret_cast<uint64_t*>(out)[k] = v;
+        else {
+            uint8_t* o = reinterpret_cast<uint8_t*>(out) + 5 * k;
             o[0] = (uint8_t)v;
             o[1] = (uint8_t)(v >> 8);
             o[2] = (uint8_t)(v >> 16);
             o[3] = (uint8_t)(v >> 24);
             o[4] = 0;
         }
+    }
+}
+
+__device__ __forceinline__ void store_sa_entry(void* out, uint64_t k, uint32_t v, int width) {
+    if (width == 32) reinterpret_cast<uint32_t*>(out)[k] = v;
+    else if (width == 64) reinterpret_cast<uint64_t*>(out)[k] = v;
+    else {
+        uint8_t* o = reinterpret_cast<uint8_t*>(out) + 5 * k;
+        o[0] = (uint8_t)v;
+        o[1] = (uint8_t)(v >> 8);
+        o[2] = (uint8_t)(v >> 16);
+        o[3] = (uint8_t)(v >> 24);
+        o[4] = 0;
+    }
+}
+
+// Several texts: sorted element k belongs to text s = segw[k]; text s's elements
+// occupy sorted slots [start[s], start[s+1]) with its empty suffix first, so
+// slot start[s] + 1 + r holds the text's r-th suffix; indices are text-local.
+__global__ void k_emit_seg(const uint32_t* __restrict__ sa_full, const uint32_t* __restrict__ segw, uint64_t N,
+                           LevelSeg ls, void* __restrict__ out, int width) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < N; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = segw[k];
+        const uint64_t r = k - ls.start[s];
+        if (r == 0) continue;
+        store_sa_entry(out, ls.obase[s] + r - 1, (uint32_t)(sa_full[k] - ls.start[s]), width);
+    }
+}
+
+__global__ void k_widen(const uint32_t* __restrict__ sa, uint64_t n, uint8_t* __restrict__ out, int width) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        store_sa_entry(out, k, sa[k], width);
+}
+
+// ---- suffix-array checker (the conditions of check_suffixarray,
+// lightweight_dcx/src/sa_check.hpp:56-184, without its sorts) ------------------
+__device__ __forceinline__ uint64_t load_sa_entry(const void* sa, uint64_t k, int width) {
+    if (width == 32) return reinterpret_cast<const uint32_t*>(sa)[k];
+    if (width == 64) return reinterpret_cast<const uint64_t*>(sa)[k];
+    const uint8_t* b = reinterpret_cast<const uint8_t*>(sa) + 5 * k;
+    return (uint64_t)b[0] | ((uint64_t)b[1] << 8) | ((uint64_t)b[2] << 16) | ((uint64_t)b[3] << 24) |
+           ((uint64_t)b[4] << 32);
+}
+
+// Permutation: every position occurs once; isa[p] = 1 + rank of suffix p.
+__global__ void k_check_isa(const void* __restrict__ sa, int width, uint64_t n, uint32_t* __restrict__ isa,
+                            unsigned long long* __restrict__ bad) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t p = load_sa_entry(sa, k, width);
+        if (p >= n) {
+            atomicAdd(bad, 1ull);
+            continue;
+        }
+        if (atomicExch(&isa[p], (uint32_t)(k + 1)) != 0u) atomicAdd(bad, 1ull);
+    }
+}
+
+// Order: for adjacent SA entries i, j: (T[i], isa[i+1]) < (T[j], isa[j+1]) with
+// isa[n] = 0 (the empty suffix is smallest).
+__global__ void k_check_order(const void* __restrict__ sa, int width, uint64_t n, const uint8_t* __restrict__ t,
+                              const uint32_t* __restrict__ isa, unsigned long long* __restrict__ bad) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; k < n;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = load_sa_entry(sa, k - 1, width), j = load_sa_entry(sa, k, width);
+        if (i >= n || j >= n) continue;  // reported by k_check_isa
+        const uint32_t ti = t[i], tj = t[j];
+        bool ok = ti < tj;
+        if (ti == tj) {
+            const uint32_t ri = i + 1 < n ? isa[i + 1] : 0u, rj = j + 1 < n ? isa[j + 1] : 0u;
+            ok = ri < rj;
+        }
+        if (!ok) atomicAdd(bad, 1ull);
     }
 }
 

@@ -30,9 +30,24 @@ struct DcDev {
     uint16_t cmp[MAX_X * MAX_X];  // r1 | r2 << 8
 };
 
+// Texts of the level: a group's elements all belong to one text s (the text id
+// is part of the sort key); the comparator works on text-local positions and
+// the text's rank slots start at rbase[s].
+struct TieSeg {
+    const uint32_t* segw;   // text of each sorted element, or null for one text
+    const uint64_t* start;  // first position of each text
+    const uint64_t* rbase;  // first rank slot of each text
+};
+
+__device__ __forceinline__ void tie_bases(const TieSeg& ts, uint64_t sorted_slot, uint64_t& pos0, uint64_t& slot0) {
+    const uint32_t s = ts.segw ? ts.segw[sorted_slot] : 0u;
+    pos0 = ts.start[s];
+    slot0 = ts.rbase[s];
+}
+
 template <int D>
 struct Rec {
-    uint32_t pos;
+    uint32_t pos;  // text-local position
     uint32_t r[D];
 };
 
@@ -90,7 +105,8 @@ __device__ __forceinline__ void load_dc_smem(const DcDev& dc, uint16_t* tab, uin
 template <int D, int W>
 __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize,
                                                   uint32_t ngroups, uint32_t* __restrict__ sa,
-                                                  const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp) {
+                                                  const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp,
+                                                  TieSeg ts) {
     __shared__ uint16_t tab[MAX_X * MAX_X];
     __shared__ uint32_t nr[MAX_X];
     load_dc_smem(*dcp, tab, nr);
@@ -101,11 +117,13 @@ __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ g
     const uint32_t l = lane % W;
     bool valid = false;
     uint32_t start = 0;
+    uint64_t pos0 = 0, slot0 = 0;
     if (g < ngroups) {
         start = gstart[g];
         valid = l < gsize[g];
+        tie_bases(ts, start, pos0, slot0);
     }
-    Rec<D> a = load_rec<D>(valid ? sa[start + l] : INVALID_POS, rank_text, X, nr);
+    Rec<D> a = load_rec<D>(valid ? (uint32_t)(sa[start + l] - pos0) : INVALID_POS, rank_text + slot0, X, nr);
 #pragma unroll
     for (int k = 2; k <= W; k <<= 1) {
 #pragma unroll
@@ -120,14 +138,14 @@ __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ g
             if (take_b) a = b;
         }
     }
-    if (valid) sa[start + l] = a.pos;
+    if (valid) sa[start + l] = (uint32_t)(a.pos + pos0);
 }
 
 // One group (or chunk) of up to C elements per CTA; bitonic network in shared memory.
 template <int D, int C, int THREADS>
 __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize,
                                                      uint32_t* __restrict__ sa, const uint32_t* __restrict__ rank_text,
-                                                     const DcDev* __restrict__ dcp) {
+                                                     const DcDev* __restrict__ dcp, TieSeg ts) {
     extern __shared__ uint32_t smem[];
     uint16_t* tab = reinterpret_cast<uint16_t*>(smem);
     uint32_t* nr = smem + (MAX_X * MAX_X + 1) / 2;
@@ -135,8 +153,10 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
     load_dc_smem(*dcp, tab, nr);
     const uint32_t X = dcp->X;
     const uint32_t start = gstart[blockIdx.x], size = gsize[blockIdx.x];
+    uint64_t pos0, slot0;
+    tie_bases(ts, start, pos0, slot0);
     for (uint32_t i = threadIdx.x; i < C; i += THREADS)
-        recs[i] = load_rec<D>(i < size ? sa[start + i] : INVALID_POS, rank_text, X, nr);
+        recs[i] = load_rec<D>(i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS, rank_text + slot0, X, nr);
     __syncthreads();
     for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -154,7 +174,7 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
             __syncthreads();
         }
     }
-    for (uint32_t i = threadIdx.x; i < size; i += THREADS) sa[start + i] = recs[i].pos;
+    for (uint32_t i = threadIdx.x; i < size; i += THREADS) sa[start + i] = (uint32_t)(recs[i].pos + pos0);
 }
 
 template <int D, int C>
@@ -169,7 +189,8 @@ template <int D>
 __global__ __launch_bounds__(256) void k_tie_merge(const uint64_t* __restrict__ offsets, uint32_t ngroups,
                                                    const uint32_t* __restrict__ gstart, uint64_t total, uint32_t w,
                                                    const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
-                                                   const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp) {
+                                                   const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp,
+                                                   TieSeg ts) {
     __shared__ uint16_t tab[MAX_X * MAX_X];
     __shared__ uint32_t nr[MAX_X];
     load_dc_smem(*dcp, tab, nr);
@@ -197,19 +218,22 @@ __global__ __launch_bounds__(256) void k_tie_merge(const uint64_t* __restrict__ 
             p_start = own_start - w;
             p_end = own_start;
         }
-        const Rec<D> me = load_rec<D>(src[base + o], rank_text, X, nr);
+        uint64_t pos0, slot0;
+        tie_bases(ts, base, pos0, slot0);
+        const uint32_t* rt = rank_text + slot0;
+        const Rec<D> me = load_rec<D>((uint32_t)(src[base + o] - pos0), rt, X, nr);
         uint64_t a = p_start, b = p_end;  // count partner elements < me
         if (p_start < size) {
             while (a < b) {
                 uint64_t mid = (a + b) >> 1;
-                Rec<D> other = load_rec<D>(src[base + mid], rank_text, X, nr);
+                Rec<D> other = load_rec<D>((uint32_t)(src[base + mid] - pos0), rt, X, nr);
                 if (dc_less<D>(other, me, X, tab)) a = mid + 1; else b = mid;
             }
         } else {
             a = p_start;
         }
         const uint64_t before = (p_start < size ? a - p_start : 0);
-        dst[base + pair_base + (o - own_start) + before] = me.pos;
+        dst[base + pair_base + (o - own_start) + before] = (uint32_t)(me.pos + pos0);
     }
 }
 

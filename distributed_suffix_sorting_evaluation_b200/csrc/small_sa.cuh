@@ -17,27 +17,29 @@ namespace dcx {
 constexpr int SMALL_MAX = 2048;
 constexpr int SMALL_THREADS = 1024;
 
-// Strings: text + offsets[s] .. offsets[s+1]; SA written at out + out_offsets[s]
-// (text-local indices).  Chars must be >= 1.
+// String s of the launch is text[start[s] .. start[s+1]-1) (each string is
+// followed by its 0); its SA (string-local indices) goes to out + obase[s].
+// Chars must be >= 1.
 template <typename CharT>
 __global__ __launch_bounds__(SMALL_THREADS) void k_small_sa(const CharT* __restrict__ text,
-                                                            const uint64_t* __restrict__ offsets,
-                                                            const uint32_t* __restrict__ ids, uint32_t* __restrict__ out) {
+                                                            const uint64_t* __restrict__ start,
+                                                            const uint64_t* __restrict__ obase, uint32_t* __restrict__ out) {
     __shared__ uint64_t key[SMALL_MAX];
     __shared__ uint16_t idx[SMALL_MAX];
     __shared__ uint32_t rank[SMALL_MAX];
     __shared__ uint32_t scan_sm[SMALL_THREADS / 32 + 1];
     __shared__ uint32_t s_done;
 
-    const uint32_t s = ids ? ids[blockIdx.x] : blockIdx.x;
-    const uint64_t b = offsets[s];
-    const uint32_t n = (uint32_t)(offsets[s + 1] - b);
+    const uint32_t s = blockIdx.x;
+    const uint64_t b = start[s];
+    const uint32_t n = (uint32_t)(start[s + 1] - b - 1);
     if (n == 0) return;
     const CharT* t = text + b;
+    out += obase[s];
     for (uint32_t i = threadIdx.x; i < n; i += SMALL_THREADS) rank[i] = (uint32_t)t[i];
     __syncthreads();
     if (n == 1) {
-        if (threadIdx.x == 0) out[b] = 0;
+        if (threadIdx.x == 0) out[0] = 0;
         return;
     }
     uint32_t C = 2;
@@ -93,7 +95,7 @@ __global__ __launch_bounds__(SMALL_THREADS) void k_small_sa(const CharT* __restr
         __syncthreads();
         if (s_done) break;
     }
-    for (uint32_t k = threadIdx.x; k < n; k += SMALL_THREADS) out[b + k] = idx[k];
+    for (uint32_t k = threadIdx.x; k < n; k += SMALL_THREADS) out[k] = idx[k];
 }
 
 }  // namespace dcx

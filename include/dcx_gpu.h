@@ -105,6 +105,14 @@ int dcx_build_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_w
 int dcx_build_sa_strict(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
                         void* sa_out, uint32_t flags);
 
+/* Checks on the GPU that sa (n entries of sa_width bits) is the suffix array of
+ * text: a permutation of 0..n-1 whose adjacent entries i, j satisfy
+ * (T[i], ISA[i+1]) < (T[j], ISA[j+1]) -- the conditions check_suffixarray
+ * establishes with distributed sorts (lightweight_dcx/src/sa_check.hpp:56-184,
+ * wired to `cli --check`, cli.cpp:700-727).  *ok = 1 if correct, 0 if not. */
+int dcx_check_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
+                 uint32_t flags, int* ok);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
  * caller can time builds with events recorded on it. */
 int dcx_get_stream(dcx_ctx* ctx, void** stream_out);
