@@ -163,6 +163,46 @@ def run_reference(args, world, rank):
     return 0
 
 
+def run_reference_batch(args, world, rank):
+    """Reference arm of the batched workload: libsais64_omp per text over a
+    bounded sample of the batch's texts (the first texts in batch order up to
+    --ref-sample-mib of text), all host threads."""
+    if rank != 0:
+        return 0
+    from distributed_suffix_sorting_evaluation_b200 import workloads as W
+    from oracle import oracle as O
+    lens = W.batch_lengths(args.batch_count, 1 << 10, 16 << 20, seed=5)
+    threads = os.cpu_count() or 1
+    cap = args.ref_sample_mib << 20
+    texts, tot = [], 0
+    for j in range(lens.size):
+        if texts and tot + int(lens[j]) > cap:
+            break
+        texts.append(W.iid(int(lens[j]), b"ACGT", seed=1_000_000 + j))
+        tot += int(lens[j])
+    O.libsais(texts[0], threads=threads)
+    vals = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        for t in texts:
+            O.libsais(t, threads=threads)
+        vals.append(tot / GiB / (time.perf_counter() - t0))
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "batched SA build GiB/s", "value": round(value, 4), "unit": "GiB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot / GiB / value * 1000, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "cfg4_batch", "texts": int(lens.size), "text_bytes": int(lens.sum()), "sa_width": 32},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GiB/s", "cores": threads, "kind": "reference",
+                         "sample": f"libsais64_omp per text on the first {len(texts)} texts "
+                                   f"({tot >> 20} MiB), {threads} threads"},
+        "e2e": {"value": round(value, 4), "unit": "GiB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gpu(args, world, rank, local):
     import torch
     from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
@@ -284,6 +324,142 @@ def run_gpu(args, world, rank, local):
     return 0
 
 
+def run_batch(args, world, rank, local):
+    """Batched workload: `count` independent i.i.d. {A,C,G,T} texts, lengths
+    log-uniform in [1 KiB, 16 MiB] (seeded), one uint32 SA per text.  The texts
+    are staged on the device a chunk (about --batch-chunk-mib of text) at a time;
+    the timed region is the batched call over every chunk with the chunk's text
+    already in HBM.  Beside it, the plain single-text call is looped over the
+    same texts (whole chunks, while --loop-budget-s lasts) and the batched time
+    of exactly those chunks gives the speed-up.  Under torchrun every rank runs
+    its own copy of the batch (replicas)."""
+    import torch
+    from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    lens = W.batch_lengths(args.batch_count, 1 << 10, 16 << 20, seed=5)
+    total = int(lens.sum())
+    # chunks of consecutive texts, each about batch_chunk_mib of text
+    cap = args.batch_chunk_mib << 20
+    chunks, s0 = [], 0
+    while s0 < lens.size:
+        s1, tot = s0, 0
+        while s1 < lens.size and (s1 == s0 or tot + int(lens[s1]) <= cap):
+            tot += int(lens[s1])
+            s1 += 1
+        chunks.append((s0, s1, tot))
+        s0 = s1
+    big = max(c[2] for c in chunks)
+    d_text = torch.empty(big + 16, dtype=torch.uint8, device=dev)
+    d_sa = torch.empty(big + 16, dtype=torch.int32, device=dev)
+    h_text = torch.empty(big + 16, dtype=torch.uint8, pin_memory=True)
+    ctx = Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def stage(ci):
+        a, b, tot = chunks[ci]
+        offs = np.zeros(b - a + 1, np.uint64)
+        offs[1:] = np.cumsum(lens[a:b], dtype=np.uint64)
+        hv = h_text.numpy()
+        for j in range(a, b):
+            o = int(offs[j - a])
+            W.iid(int(lens[j]), b"ACGT", seed=1_000_000 + j + 7919 * rank, out=hv[o:o + int(lens[j])])
+        d_text[:tot].copy_(h_text[:tot], non_blocking=True)
+        torch.cuda.synchronize()
+        return offs
+
+    def batched(offs):
+        ctx.build_sa_batch_raw(d_text.data_ptr(), offs.ctypes.data, offs.size - 1, d_sa.data_ptr(), dc=0,
+                               sa_width=32, device=True)
+
+    def looped(offs):
+        for k in range(offs.size - 1):
+            b, n = int(offs[k]), int(offs[k + 1] - offs[k])
+            ctx.build_sa_device(d_text.data_ptr() + b, n, d_sa.data_ptr() + 4 * b, dc=39, sa_width=32)
+
+    offs0 = stage(0)
+    for _ in range(max(1, args.warmup)):
+        batched(offs0)
+    torch.cuda.synchronize()
+    batch_ms, loop_ms, loop_batch_ms = [], 0.0, 0.0
+    loop_texts = loop_bytes = 0
+    launches = 0
+    verified = 0
+    loop_open = args.loop_budget_s > 0
+    with ClockSampler(local) as clocks:
+        for ci in range(len(chunks)):
+            offs = offs0 if ci == 0 else stage(ci)
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            batched(offs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            batch_ms.append(ms)
+            launches += ctx.stats()["kernel_launches"]
+            if args.verify:
+                a, b, tot = chunks[ci]
+                for k in sorted({0, (b - a) // 2, b - a - 1}):
+                    o, n = int(offs[k]), int(offs[k + 1] - offs[k])
+                    t = h_text.numpy()[o:o + n].copy()
+                    raw = d_sa[o:o + n].cpu().numpy().view(np.uint8)
+                    if not ctx.check_sa(t, raw, 32):
+                        raise SystemExit(f"batched SA of text {a + k} failed the check")
+                    verified += 1
+            if loop_open:
+                e0.record(stream)
+                looped(offs)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                loop_ms += e0.elapsed_time(e1)
+                loop_batch_ms += ms
+                loop_texts += chunks[ci][1] - chunks[ci][0]
+                loop_bytes += chunks[ci][2]
+                loop_open = loop_ms < args.loop_budget_s * 1000.0
+    clock = clocks.summary()
+    ms_total = sum(batch_ms)
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+    value = world * total / GiB / (ms_total / 1000.0)
+    if rank == 0:
+        loop_v = loop_bytes / GiB / (loop_ms / 1000.0) if loop_ms > 0 else None
+        same_v = loop_bytes / GiB / (loop_batch_ms / 1000.0) if loop_batch_ms > 0 else None
+        line = {
+            "metric": "batched SA build GiB/s", "value": round(value, 4), "unit": "GiB/s", "n_gpus": world,
+            "steps": len(chunks), "warmup": max(1, args.warmup), "ms_per_step": round(ms_total / len(chunks), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded i.i.d. {A,C,G,T} texts, log-uniform lengths 1 KiB-16 MiB)",
+            "config": {"workload": "cfg4_batch", "texts": int(lens.size), "text_bytes": total,
+                       "chunk_mib": args.batch_chunk_mib, "dc": "auto per text", "sa_width": 32,
+                       "l2_flush": "each chunk's text and SAs are larger than L2",
+                       "parallelism": "replicas" if world > 1 else "single-gpu"},
+            "seconds": round(ms_total / 1000.0, 3),
+            "loop": {"value": None if loop_v is None else round(loop_v, 4), "unit": "GiB/s", "texts": loop_texts,
+                     "bytes": loop_bytes, "call": "dcx_build_sa per text, DC39, device pointers",
+                     "batched_same_texts": None if same_v is None else round(same_v, 4),
+                     "speedup": None if not (loop_v and same_v) else round(same_v / loop_v, 3)},
+            "verified_texts": verified,
+            "gpu_launches": int(launches),
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -296,8 +472,16 @@ def main():
     ap.add_argument("--cpu-sample-mib", type=int, default=256)
     ap.add_argument("--ref-sample-mib", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
+    ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
+    ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")
+    ap.add_argument("--verify", action="store_true", help="check three SAs of every batched chunk on the GPU")
     args = ap.parse_args()
     world, rank, local = _dist()
+    if args.workload == "cfg4_batch":
+        if args.impl == "reference":
+            return run_reference_batch(args, world, rank)
+        return run_batch(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     return run_gpu(args, world, rank, local)

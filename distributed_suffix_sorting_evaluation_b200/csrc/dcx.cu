@@ -127,15 +127,23 @@ struct BigUInt {  // little-endian 32-bit limbs
     }
 };
 
-static uint32_t key_bits(uint64_t B, uint32_t P) {
+// Bits of the largest key K * B^P - 1 (K texts, P chars of base B).
+static uint32_t key_bits_k(uint64_t B, uint32_t P, uint64_t K) {
     BigUInt x;
+    if (K > 1) {
+        x.mul((uint32_t)(K & 0xffffffffu));
+        if (K >> 32) throw Error(DCX_ERR_ARG, "too many texts");
+    }
     for (uint32_t i = 0; i < P; i++) x.mul((uint32_t)B);
     return std::max<uint32_t>(1, x.bits_of_minus_one());
 }
 
-static uint32_t max_chars_in_bits(uint64_t B, uint32_t bits) {
+// Largest P with K * B^P - 1 < 2^bits.
+static uint32_t max_chars_in_bits_k(uint64_t B, uint32_t bits, uint64_t K) {
     uint32_t P = 0;
     BigUInt x;
+    if (K > 1) x.mul((uint32_t)K);
+    if (x.bits_of_minus_one() > bits) return 0;
     while (true) {
         BigUInt y = x;
         y.mul((uint32_t)B);
@@ -147,13 +155,16 @@ static uint32_t max_chars_in_bits(uint64_t B, uint32_t bits) {
     return P;
 }
 
+static uint32_t max_chars_in_bits(uint64_t B, uint32_t bits) { return max_chars_in_bits_k(B, bits, 1); }
 static uint32_t max_chars_in(uint64_t B, uint32_t words) { return max_chars_in_bits(B, 32 * words); }
 
-static KeyPlan make_plan(uint64_t B, uint32_t P) {
+// Chunked encoding of P chars of base B; the key words also hold a text id
+// digit (0..K-1) above the chars.
+static KeyPlan make_plan(uint64_t B, uint32_t P, uint64_t K = 1) {
     KeyPlan p{};
     p.base = (uint32_t)B;
     p.chars = P;
-    p.kw = (key_bits(B, P) + 31) / 32;
+    p.kw = (key_bits_k(B, P, K) + 31) / 32;
     uint32_t kmax = 1;
     {
         uint64_t v = B;
@@ -180,6 +191,8 @@ static KeyPlan make_plan(uint64_t B, uint32_t P) {
 // ---------------------------------------------------------------------------
 // Context: stream, memory accounting, scratch, options, statistics.
 // ---------------------------------------------------------------------------
+constexpr size_t PINNED_WORDS = 1 << 14;  // 64 KiB: two 16-pass x 256-bin tables
+
 struct Options {
     double discarding_threshold = 0.7;
     uint32_t recursion_dc = 3;
@@ -224,7 +237,7 @@ struct Ctx {
     uint64_t* d_lookback = nullptr;
     size_t lookback_tiles = 0;
     uint32_t epoch = 0;
-    uint32_t* h_pinned = nullptr;   // pinned staging for small D2H
+    uint32_t* h_pinned = nullptr;   // pinned staging for small transfers (PINNED_WORDS words)
     std::map<uint32_t, DcHost> dc_host;
     std::map<uint32_t, DcFlags*> dc_flags_dev;  // per X (samples_before filled per level on a copy)
     std::map<uint32_t, DcDev*> dc_dev;
@@ -288,12 +301,13 @@ static int grid_for(uint64_t n, int threads, int max_blocks = 148 * 16) {
     return (int)std::min<uint64_t>(b, (uint64_t)max_blocks);
 }
 
+// Small device->host reads go through the context's pinned staging area.
 template <typename T>
 static T d2h_scalar(Ctx& c, const T* dptr) {
-    T v;
-    DCX_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    T* h = reinterpret_cast<T*>(c.h_pinned);
+    DCX_CUDA(cudaMemcpyAsync(h, dptr, sizeof(T), cudaMemcpyDeviceToHost, c.stream));
     DCX_CUDA(cudaStreamSynchronize(c.stream));
-    return v;
+    return *h;
 }
 
 static void check_device_error(Ctx& c) {
@@ -353,8 +367,10 @@ struct SortSpace {
 
 static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
     const uint32_t passes = 4 * kw;
-    std::vector<uint32_t> h((size_t)passes * RADIX);
-    DCX_CUDA(cudaMemcpyAsync(h.data(), c.d_hist, h.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+    // histograms in and digit bases out through pinned staging (PINNED_WORDS words each)
+    uint32_t* h = reinterpret_cast<uint32_t*>(c.h_pinned);
+    uint32_t* hb = h + PINNED_WORDS / 2;
+    DCX_CUDA(cudaMemcpyAsync(h, c.d_hist, (size_t)passes * RADIX * 4, cudaMemcpyDeviceToHost, c.stream));
     DCX_CUDA(cudaStreamSynchronize(c.stream));
     std::vector<uint32_t> run;
     std::vector<uint32_t> bases;
@@ -382,7 +398,8 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         c.lookback_tiles = want;
         c.epoch = 0;
     }
-    DCX_CUDA(cudaMemcpyAsync(c.d_base, bases.data(), bases.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    std::copy(bases.begin(), bases.end(), hb);
+    DCX_CUDA(cudaMemcpyAsync(c.d_base, hb, bases.size() * 4, cudaMemcpyHostToDevice, c.stream));
     DCX_CUDA(cudaMemsetAsync(c.d_tiles, 0, run.size() * 4, c.stream));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -460,9 +477,9 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     const uint32_t K = sg.K();
     const bool SEGK = K > 1;
     const SegView sv{K, d_start};
-    const uint32_t words_full = (key_bits(B, L) + 31) / 32;
+    const uint32_t words_full = (key_bits_k(B, L, K) + 31) / 32;
     uint32_t kw0_max = depth == 0 ? 2 : 3;
-    uint32_t P0 = std::min<uint32_t>(L, max_chars_in(B, std::min(words_full, kw0_max)));
+    uint32_t P0 = std::min<uint32_t>(L, max_chars_in_bits_k(B, 32 * std::min(words_full, kw0_max), K));
     if (depth == 0 && c.level0_entropy > 0.05) {
         // Shortest byte-aligned prefix whose expected random collisions stay near
         // 1% of N: P * H >= log2(N) + 7, with H the order-0 entropy discounted by
@@ -471,20 +488,20 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         const double need = std::log2((double)N) + 7.0;
         uint32_t P = (uint32_t)std::ceil(need / (0.85 * c.level0_entropy));
         P = std::max<uint32_t>(1, std::min(P, P0));
-        const uint32_t bytes = (key_bits(B, P) + 7) / 8;
-        const uint32_t fill = std::min<uint32_t>(P0, max_chars_in_bits(B, 8 * bytes));
+        const uint32_t bytes = (key_bits_k(B, P, K) + 7) / 8;
+        const uint32_t fill = std::min<uint32_t>(P0, max_chars_in_bits_k(B, 8 * bytes, K));
         P0 = std::max(P, fill);
     }
     if (c.opt.prefix_chars && depth == 0) P0 = std::min<uint32_t>(L, c.opt.prefix_chars);
     if (P0 == 0) P0 = 1;
-    KeyPlan plan = make_plan(B, P0);
+    KeyPlan plan = make_plan(B, P0, K);  // key = text id * B^P0 + window
     if (plan.kw > 3) throw Error(DCX_ERR_INTERNAL, "prefix key wider than 3 words");
     const uint32_t kw = plan.kw;
-    const uint32_t kwt = kw + (SEGK ? 1u : 0u);  // + text id word
+    const uint32_t kwt = kw;
 
     // round 0
     {
-        DBuf<uint32_t> keys[2][4];
+        DBuf<uint32_t> keys[2][3];
         DBuf<uint32_t> vals[2];
         SortSpace s;
         for (int b = 0; b < 2; b++) {
@@ -504,14 +521,17 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
             // sliding-window builder: keys of consecutive positions share P-1 chars
             uint64_t pow_top = 1;
             for (uint32_t i = 1; i < P0; i++) pow_top *= B;
+            const uint64_t seg_mul = pow_top * B;  // B^P0: weight of the text id digit
             const size_t sshm = keys_slide_smem<CharT>();
             const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 2);
             if (SEGK) {
                 DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<true, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
-                k_keys_slide<true, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, ko, s.v[0], c.d_hist);
+                k_keys_slide<true, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, seg_mul,
+                                                                                    ko, s.v[0], c.d_hist);
             } else {
                 DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<false, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
-                k_keys_slide<false, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, ko, s.v[0], c.d_hist);
+                k_keys_slide<false, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, seg_mul,
+                                                                                     ko, s.v[0], c.d_hist);
             }
         } else {
 #define DCX_PREFIX(KWV, SEGV)                                                                                       \
@@ -537,7 +557,14 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         c.launched();
         c.alg(N * kwt * 4 + N);
         sa = std::move(vals[f]);
-        if (SEGK) segw = std::move(keys[f][kwt - 1]);
+        if (SEGK) {
+            // the sort is text-major, so text s owns sorted slots [start[s], start[s+1])
+            segw = DBuf<uint32_t>(&c, N);
+            k_fill_segw<<<grid_for(div_up(N, 16), 256), 256, 0, c.stream>>>(sv, N, segw.get());
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            c.alg(N * 4);
+        }
     }
 
     // refinement rounds for tied windows (a group never spans two texts)
@@ -1232,7 +1259,6 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
             tot += offsets[s1 + 1] - offsets[s1] + 1;
             s1++;
         }
-        const uint32_t Kr = s1 - s0;
         const uint64_t in_bytes = offsets[s1] - offsets[s0];
         // input of the round on the device (one copy)
         DBuf<uint8_t> din;
@@ -1303,30 +1329,33 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
         auto run_group = [&](const Segs& g, const std::vector<uint32_t>& ids) {
             if (ids.empty()) return;
             const uint32_t Kg = g.K();
-            std::vector<uint64_t> goff(Kg + 1, 0), gsrc(Kg);
+            std::vector<uint64_t> goff(Kg + 1, 0), gsrc(Kg), cbase(Kg + 1, 0);
             for (uint32_t k = 0; k < Kg; k++) {
+                const uint64_t len = in_off[ids[k] + 1] - in_off[ids[k]];
                 gsrc[k] = in_off[ids[k]];
-                goff[k + 1] = goff[k] + (in_off[ids[k] + 1] - in_off[ids[k]]);
+                goff[k + 1] = goff[k] + len;
+                cbase[k + 1] = cbase[k] + std::max<uint64_t>(1, div_up(len, TEXT_CHUNK));
             }
-            DBuf<uint64_t> d_goff = upload(c, goff), d_gsrc = upload(c, gsrc);
+            DBuf<uint64_t> d_goff = upload(c, goff), d_gsrc = upload(c, gsrc), d_cbase = upload(c, cbase);
             const uint64_t Ng = g.N();
+            const uint64_t chunks = cbase[Kg];
             DBuf<uint8_t> gout(&c, std::max<uint64_t>(goff[Kg], 1) * wb + 16);
-            const uint32_t blocks = std::min<uint32_t>(Kg, 65535);
+            const uint32_t blocks = (uint32_t)std::min<uint64_t>(chunks, 148 * 16);
             if (wide) {
                 DBuf<uint32_t> buf(&c, Ng + 1);
-                k_spread_texts<uint32_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), Kg, buf.get(),
-                                                                       d_map.get(), true);
+                k_spread_texts<uint32_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), d_cbase.get(),
+                                                                       Kg, chunks, buf.get(), d_map.get(), true);
                 DCX_CHECK_LAUNCH();
                 level<uint32_t>(c, buf.get(), g, sigma, X, 0, packing, gout.get(), width);
             } else {
                 DBuf<uint8_t> buf(&c, Ng + 16);
-                k_spread_texts<uint8_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), Kg, buf.get(),
-                                                                      d_map.get(), false);
+                k_spread_texts<uint8_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), d_cbase.get(),
+                                                                      Kg, chunks, buf.get(), d_map.get(), false);
                 DCX_CHECK_LAUNCH();
                 level<uint8_t>(c, buf.get(), g, sigma, X, 0, packing, gout.get(), width);
             }
-            k_scatter_outputs<<<blocks, 256, 0, c.stream>>>(gout.get(), d_gsrc.get(), d_goff.get(), Kg, rout,
-                                                           (uint32_t)wb);
+            k_scatter_outputs<<<blocks, 256, 0, c.stream>>>(gout.get(), d_gsrc.get(), d_goff.get(), d_cbase.get(), Kg,
+                                                           chunks, rout, (uint32_t)wb);
             DCX_CHECK_LAUNCH();
             c.launched(2);
         };
@@ -1456,6 +1485,7 @@ int dcx_ctx_create(dcx_ctx** out, int device, uint64_t budget) {
             DCX_CUDA(cudaMalloc(&c.d_err, 4));
             DCX_CUDA(cudaMemset(c.d_err, 0, 4));
             DCX_CUDA(cudaMalloc(&c.d_h256, 256 * 8));
+            DCX_CUDA(cudaHostAlloc((void**)&c.h_pinned, dcx::PINNED_WORDS * 4, cudaHostAllocDefault));
         } catch (...) {
             delete x;
             throw;
@@ -1476,6 +1506,7 @@ int dcx_ctx_destroy(dcx_ctx* x) {
         cudaFree(c.d_err);
         cudaFree(c.d_h256);
         if (c.d_lookback) cudaFree(c.d_lookback);
+        if (c.h_pinned) cudaFreeHost(c.h_pinned);
         for (auto& kv : c.dc_dev) cudaFree(kv.second);
         if (c.stream) cudaStreamDestroy(c.stream);
         delete x;

@@ -40,9 +40,10 @@ __device__ __forceinline__ uint32_t ldc(const CharT* p) {
 // Encodes chars text[start .. start+plan.chars) (0 at or past `end`) into acc[0..KW).
 template <int KW, typename CharT>
 __device__ __forceinline__ void encode_window(const CharT* text, uint64_t end, uint64_t start,
-                                              const KeyPlan& plan, uint32_t* acc) {
+                                              const KeyPlan& plan, uint32_t* acc, uint32_t top = 0) {
 #pragma unroll
     for (int w = 0; w < KW; w++) acc[w] = 0;
+    acc[0] = top;  // most significant digit (text id), scaled up by the chunk multiplies
     uint64_t p = start;
     for (uint32_t c = 0; c < plan.nchunks; c++) {
         const uint32_t len = plan.chunk_len[c];
@@ -116,26 +117,25 @@ __device__ __forceinline__ uint32_t seg_of(const SegView& sv, uint64_t p) {
 }
 __device__ __forceinline__ uint64_t seg_end(const SegView& sv, uint32_t s) { return sv.start[s + 1] - 1; }
 
-// Level keys: for every position i in [0, N), key = window [i, i+chars) of i's
-// text, value = i; with K > 1 the text id is one more, most significant, word.
+// Level keys: for every position i in [0, N), key = text * B^chars + window
+// [i, i+chars) of i's text (the text id is the most significant mixed-radix
+// digit), value = i.
 template <int KW, bool SEG, typename CharT>
 __global__ __launch_bounds__(256) void k_keys_prefix(const CharT* __restrict__ text, uint64_t N, SegView sv,
                                                      KeyPlan plan, KeyOut ko, uint32_t* __restrict__ vals_out,
                                                      uint32_t* hist) {
-    constexpr int W = KW + (SEG ? 1 : 0);
-    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*W * RADIX
-    hist_zero(sh, 4 * W * RADIX);
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*KW * RADIX
+    hist_zero(sh, 4 * KW * RADIX);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t sg = SEG ? seg_of(sv, i) : 0u;
-        uint32_t key[W];
-        encode_window<KW>(text, seg_end(sv, sg), i, plan, key);
-        if (SEG) key[W - 1] = sg;
+        uint32_t key[KW];
+        encode_window<KW>(text, seg_end(sv, sg), i, plan, key, sg);  // key = text * B^P + window
 #pragma unroll
-        for (int w = 0; w < W; w++) ko.w[w][i] = key[w];
+        for (int w = 0; w < KW; w++) ko.w[w][i] = key[w];
         vals_out[i] = (uint32_t)i;
-        hist_add<W>(sh, key);
+        hist_add<KW>(sh, key);
     }
-    hist_flush(sh, 4 * W * RADIX, hist);
+    hist_flush(sh, 4 * KW * RADIX, hist);
 }
 
 // Level keys for windows of at most 64 bits, built with a sliding window: a CTA
@@ -151,14 +151,14 @@ constexpr int SLIDE_MAX_CHARS = 64;
 
 template <bool SEG, typename CharT>
 __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __restrict__ text, uint64_t N, SegView sv,
-                                                              KeyPlan plan, uint64_t pow_top, KeyOut ko,
-                                                              uint32_t* __restrict__ vals_out, uint32_t* hist) {
-    extern __shared__ uint32_t sh[];  // HIST_COPIES * 12 * RADIX histogram words, then the staging area
+                                                              KeyPlan plan, uint64_t pow_top, uint64_t seg_mul,
+                                                              KeyOut ko, uint32_t* __restrict__ vals_out,
+                                                              uint32_t* hist) {
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 8 * RADIX histogram words, then the staging area
     uint32_t* hst = sh;
-    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 12 * RADIX);  // SLIDE_TILE keys
-    uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_keys + SLIDE_TILE);             // SLIDE_TILE text ids
-    CharT* s_chars = reinterpret_cast<CharT*>(s_seg + SLIDE_TILE);                  // SLIDE_TILE + P chars
-    const uint32_t W = plan.kw + (SEG ? 1 : 0);
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 8 * RADIX);  // SLIDE_TILE keys
+    CharT* s_chars = reinterpret_cast<CharT*>(s_keys + SLIDE_TILE);                // SLIDE_TILE + P chars
+    const uint32_t W = plan.kw;
     hist_zero(hst, 4 * W * RADIX);
     const uint32_t P = plan.chars;
     const uint64_t B = plan.base;
@@ -180,8 +180,7 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
 #pragma unroll
         for (int r = 0; r < SLIDE_R; r++) {
             const uint64_t i = base + r0 + r;
-            s_keys[r0 + r] = key;
-            if (SEG) s_seg[r0 + r] = sg;
+            s_keys[r0 + r] = SEG ? key + (uint64_t)sg * seg_mul : key;  // text * B^P + window
             if (i == end) {  // next position starts the next text
                 if (SEG && sg + 1 < sv.K) {
                     sg++;
@@ -198,16 +197,11 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
         const uint32_t tile_n = (uint32_t)((N - base) < SLIDE_TILE ? (N - base) : SLIDE_TILE);
         for (uint32_t i = threadIdx.x; i < tile_n; i += SLIDE_THREADS) {
             const uint64_t k = s_keys[i];
-            uint32_t kk[3] = {(uint32_t)k, (uint32_t)(k >> 32), 0u};
+            uint32_t kk[2] = {(uint32_t)k, (uint32_t)(k >> 32)};
             ko.w[0][base + i] = kk[0];
-            if (plan.kw > 1) ko.w[1][base + i] = kk[1];
-            if (SEG) {
-                kk[plan.kw] = s_seg[i];
-                ko.w[plan.kw][base + i] = s_seg[i];
-            }
+            if (W > 1) ko.w[1][base + i] = kk[1];
             vals_out[base + i] = (uint32_t)(base + i);
-            if (W == 3) hist_add<3>(hst, kk);
-            else if (W == 2) hist_add<2>(hst, kk);
+            if (W == 2) hist_add<2>(hst, kk);
             else hist_add<1>(hst, kk);
         }
         __syncthreads();
@@ -217,8 +211,23 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
 
 template <typename CharT>
 constexpr size_t keys_slide_smem() {
-    return sizeof(uint32_t) * HIST_COPIES * 12 * RADIX + sizeof(uint64_t) * SLIDE_TILE + sizeof(uint32_t) * SLIDE_TILE +
+    return sizeof(uint32_t) * HIST_COPIES * 8 * RADIX + sizeof(uint64_t) * SLIDE_TILE +
            sizeof(CharT) * (SLIDE_TILE + SLIDE_MAX_CHARS);
+}
+
+// Text id of every sorted element: the key is text-major and text s has
+// start[s+1] - start[s] elements, so it owns sorted slots [start[s], start[s+1]).
+// One binary search per thread, then a run of consecutive slots.
+__global__ void k_fill_segw(SegView sv, uint64_t N, uint32_t* __restrict__ segw) {
+    constexpr uint32_t RUN = 16;
+    for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * RUN; b < N;
+         b += (uint64_t)gridDim.x * blockDim.x * RUN) {
+        uint32_t s = seg_of(sv, b);
+        for (uint64_t k = b; k < b + RUN && k < N; k++) {
+            while (k >= sv.start[s + 1]) s++;
+            segw[k] = s;
+        }
+    }
 }
 
 // Refinement keys for the elements of tie groups: element j has text position

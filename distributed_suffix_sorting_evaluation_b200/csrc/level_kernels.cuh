@@ -110,35 +110,57 @@ __global__ void k_widen_text(const uint8_t* __restrict__ in, uint64_t n, uint32_
 
 // Batch layout: text k of a group (src_off[k] in the round input, length
 // goff[k+1] - goff[k]) moves to goff[k] + k of the level buffer, leaving one 0
-// after every text.  A thread block per text; `widen` maps byte b to the
+// after every text.  Texts are cut into chunks of TEXT_CHUNK chars (at least
+// one per text, so empty texts still get their 0): text k owns chunks
+// [cbase[k], cbase[k+1]), and a thread block handles one chunk at a time, so
+// one long text does not serialise the launch.  `widen` maps byte b to the
 // 32-bit char b + 1, otherwise the round's alphabet map applies.
+constexpr uint32_t TEXT_CHUNK = 16384;
+
+__device__ __forceinline__ uint32_t chunk_text(const uint64_t* cbase, uint32_t K, uint64_t chunk) {
+    uint32_t lo = 0, hi = K;  // largest k with cbase[k] <= chunk
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (cbase[mid] <= chunk) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 template <typename CharT>
 __global__ void k_spread_texts(const uint8_t* __restrict__ in, const uint64_t* __restrict__ src_off,
-                               const uint64_t* __restrict__ goff, uint32_t K, CharT* __restrict__ out,
-                               const ByteMap* __restrict__ map, bool widen) {
+                               const uint64_t* __restrict__ goff, const uint64_t* __restrict__ cbase, uint32_t K,
+                               uint64_t chunks, CharT* __restrict__ out, const ByteMap* __restrict__ map,
+                               bool widen) {
     __shared__ uint8_t m[256];
     if (!widen)
         for (int i = threadIdx.x; i < 256; i += blockDim.x) m[i] = map->m[i];
     __syncthreads();
-    for (uint32_t k = blockIdx.x; k < K; k += gridDim.x) {
+    for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const uint32_t k = chunk_text(cbase, K, c);
         const uint64_t len = goff[k + 1] - goff[k];
+        const uint64_t lo = (c - cbase[k]) * TEXT_CHUNK;
+        const uint64_t hi = lo + TEXT_CHUNK < len ? lo + TEXT_CHUNK : len;
         const uint8_t* src = in + src_off[k];
         CharT* o = out + goff[k] + k;
-        for (uint64_t i = threadIdx.x; i < len; i += blockDim.x)
+        for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
             o[i] = widen ? (CharT)((uint32_t)src[i] + 1u) : (CharT)m[src[i]];
-        if (threadIdx.x == 0) o[len] = CharT(0);
+        if (hi == len && threadIdx.x == 0) o[len] = CharT(0);
     }
 }
 
 // Group outputs (goff layout, wb bytes per entry) to the texts' slots in the
-// round's output (src_off layout).
+// round's output (src_off layout), by the same chunks as k_spread_texts.
 __global__ void k_scatter_outputs(const uint8_t* __restrict__ gout, const uint64_t* __restrict__ src_off,
-                                  const uint64_t* __restrict__ goff, uint32_t K, uint8_t* __restrict__ out, uint32_t wb) {
-    for (uint32_t k = blockIdx.x; k < K; k += gridDim.x) {
-        const uint64_t bytes = (goff[k + 1] - goff[k]) * wb;
+                                  const uint64_t* __restrict__ goff, const uint64_t* __restrict__ cbase, uint32_t K,
+                                  uint64_t chunks, uint8_t* __restrict__ out, uint32_t wb) {
+    for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const uint32_t k = chunk_text(cbase, K, c);
+        const uint64_t len = goff[k + 1] - goff[k];
+        const uint64_t lo = (c - cbase[k]) * TEXT_CHUNK;
+        const uint64_t hi = lo + TEXT_CHUNK < len ? lo + TEXT_CHUNK : len;
         const uint8_t* src = gout + goff[k] * wb;
         uint8_t* dst = out + src_off[k] * wb;
-        for (uint64_t i = threadIdx.x; i < bytes; i += blockDim.x) dst[i] = src[i];
+        for (uint64_t i = lo * wb + threadIdx.x; i < hi * wb; i += blockDim.x) dst[i] = src[i];
     }
 }
 
