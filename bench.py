@@ -405,7 +405,8 @@ def run_batch(args, world, rank, local):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1)
             batch_ms.append(ms)
-            launches += ctx.stats()["kernel_launches"]
+            last_stats = ctx.stats()
+            launches += last_stats["kernel_launches"]
             if args.verify:
                 a, b, tot = chunks[ci]
                 for k in sorted({0, (b - a) // 2, b - a - 1}):
@@ -451,6 +452,7 @@ def run_batch(args, world, rank, local):
                      "speedup": None if not (loop_v and same_v) else round(same_v / loop_v, 3)},
             "verified_texts": verified,
             "gpu_launches": int(launches),
+            "build_stats_last_chunk": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in last_stats.items()},
             "clocks": clock,
         }
         print(json.dumps(line), flush=True)

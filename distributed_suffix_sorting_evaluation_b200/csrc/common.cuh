@@ -166,4 +166,18 @@ __global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(Op op, uint64_t n, 
     }
 }
 
+// SA entry k of an output of `width` bits (32, 64, or 40 = 5 little-endian bytes).
+__device__ __forceinline__ void store_sa_entry(void* out, uint64_t k, uint32_t v, int width) {
+    if (width == 32) reinterpret_cast<uint32_t*>(out)[k] = v;
+    else if (width == 64) reinterpret_cast<uint64_t*>(out)[k] = v;
+    else {
+        uint8_t* o = reinterpret_cast<uint8_t*>(out) + 5 * k;
+        o[0] = (uint8_t)v;
+        o[1] = (uint8_t)(v >> 8);
+        o[2] = (uint8_t)(v >> 16);
+        o[3] = (uint8_t)(v >> 24);
+        o[4] = 0;
+    }
+}
+
 }  // namespace dcx

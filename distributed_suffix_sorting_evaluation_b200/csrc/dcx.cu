@@ -452,7 +452,8 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
 // start[s+1]-1) of the level buffer, followed by one 0 (its empty suffix).
 // ---------------------------------------------------------------------------
 struct Segs {
-    std::vector<uint64_t> start;  // K + 1 entries, start[K] = N
+    std::vector<uint64_t> start;     // K + 1 entries, start[K] = N
+    std::vector<uint64_t> out_base;  // level 0 only, optional [K]: first output entry of text s (default packed)
     uint32_t K() const { return (uint32_t)start.size() - 1; }
     uint64_t N() const { return start.back(); }
     uint64_t len(uint32_t s) const { return start[s + 1] - start[s] - 1; }
@@ -523,7 +524,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
             for (uint32_t i = 1; i < P0; i++) pow_top *= B;
             const uint64_t seg_mul = pow_top * B;  // B^P0: weight of the text id digit
             const size_t sshm = keys_slide_smem<CharT>();
-            const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 2);
+            const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 3);  // 3 CTAs per SM by smem
             if (SEGK) {
                 DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<true, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
                 k_keys_slide<true, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, seg_mul,
@@ -560,7 +561,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         if (SEGK) {
             // the sort is text-major, so text s owns sorted slots [start[s], start[s+1])
             segw = DBuf<uint32_t>(&c, N);
-            k_fill_segw<<<grid_for(div_up(N, 16), 256), 256, 0, c.stream>>>(sv, N, segw.get());
+            k_fill_segw<<<grid_for(div_up(N, FILL_TILE), 1, 148 * 8), 256, 0, c.stream>>>(sv, N, segw.get());
             DCX_CHECK_LAUNCH();
             c.launched();
             c.alg(N * 4);
@@ -756,24 +757,16 @@ static void small_sa_batch(Ctx& c, const void* text, bool wide, const Segs& sg, 
     const uint32_t K = sg.K();
     std::vector<uint64_t> obase(K + 1, 0);
     for (uint32_t s = 0; s < K; s++) obase[s + 1] = obase[s] + sg.len(s);
+    if (!sg.out_base.empty()) std::copy(sg.out_base.begin(), sg.out_base.end(), obase.begin());
     DBuf<uint64_t> dst = upload(c, sg.start), dob = upload(c, obase);
-    DBuf<uint32_t> tmp;
-    uint32_t* o32 = (uint32_t*)out;
-    if (out_width != 32) {
-        tmp = DBuf<uint32_t>(&c, std::max<uint64_t>(obase[K], 1));
-        o32 = tmp.get();
-    }
     for (uint32_t b = 0; b < K; b += 65535) {
         const uint32_t nb = std::min<uint32_t>(K - b, 65535);
         if (wide)
-            k_small_sa<uint32_t><<<nb, SMALL_THREADS, 0, c.stream>>>((const uint32_t*)text, dst.get() + b, dob.get() + b, o32);
+            k_small_sa<uint32_t><<<nb, SMALL_THREADS, 0, c.stream>>>((const uint32_t*)text, dst.get() + b, dob.get() + b,
+                                                                      out, out_width);
         else
-            k_small_sa<uint8_t><<<nb, SMALL_THREADS, 0, c.stream>>>((const uint8_t*)text, dst.get() + b, dob.get() + b, o32);
-        DCX_CHECK_LAUNCH();
-        c.launched();
-    }
-    if (out_width != 32) {
-        k_widen<<<grid_for(obase[K], 256), 256, 0, c.stream>>>(o32, obase[K], (uint8_t*)out, out_width);
+            k_small_sa<uint8_t><<<nb, SMALL_THREADS, 0, c.stream>>>((const uint8_t*)text, dst.get() + b, dob.get() + b,
+                                                                     out, out_width);
         DCX_CHECK_LAUNCH();
         c.launched();
     }
@@ -831,6 +824,7 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
         qbase[s + 1] = qbase[s] + m;
         obase[s + 1] = obase[s] + n;
     }
+    if (!sg.out_base.empty()) std::copy(sg.out_base.begin(), sg.out_base.end(), obase.begin());
     const uint64_t m = qbase[K];
     const uint64_t slots = rbase[K];
     if (m >= (1ull << 31)) throw Error(DCX_ERR_ARG, "more than 2^31 samples in one level");
@@ -1060,10 +1054,10 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
     tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc, TieSeg{segw_p, d_start.get(), d_rbase.get()});
     head.reset();
     rank_text.reset();
-    if (K == 1) {
+    if (K == 1 && sg.out_base.empty()) {
         k_emit<<<grid_for(N / 4 + 1, 256), 256, 0, c.stream>>>(sa.get(), N - 1, sa_out, out_width);
     } else {
-        k_emit_seg<<<grid_for(N, 256), 256, 0, c.stream>>>(sa.get(), segw.get(), N, ls, sa_out, out_width);
+        k_emit_seg<<<grid_for(N, 256), 256, 0, c.stream>>>(sa.get(), segw_p, N, ls, sa_out, out_width);
     }
     DCX_CHECK_LAUNCH();
     c.launched();
@@ -1339,25 +1333,23 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
             DBuf<uint64_t> d_goff = upload(c, goff), d_gsrc = upload(c, gsrc), d_cbase = upload(c, cbase);
             const uint64_t Ng = g.N();
             const uint64_t chunks = cbase[Kg];
-            DBuf<uint8_t> gout(&c, std::max<uint64_t>(goff[Kg], 1) * wb + 16);
+            Segs gd = g;  // each text's SA goes straight to its slot of the round output
+            gd.out_base = gsrc;
             const uint32_t blocks = (uint32_t)std::min<uint64_t>(chunks, 148 * 16);
             if (wide) {
                 DBuf<uint32_t> buf(&c, Ng + 1);
                 k_spread_texts<uint32_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), d_cbase.get(),
                                                                        Kg, chunks, buf.get(), d_map.get(), true);
                 DCX_CHECK_LAUNCH();
-                level<uint32_t>(c, buf.get(), g, sigma, X, 0, packing, gout.get(), width);
+                level<uint32_t>(c, buf.get(), gd, sigma, X, 0, packing, rout, width);
             } else {
                 DBuf<uint8_t> buf(&c, Ng + 16);
                 k_spread_texts<uint8_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), d_cbase.get(),
                                                                       Kg, chunks, buf.get(), d_map.get(), false);
                 DCX_CHECK_LAUNCH();
-                level<uint8_t>(c, buf.get(), g, sigma, X, 0, packing, gout.get(), width);
+                level<uint8_t>(c, buf.get(), gd, sigma, X, 0, packing, rout, width);
             }
-            k_scatter_outputs<<<blocks, 256, 0, c.stream>>>(gout.get(), d_gsrc.get(), d_goff.get(), d_cbase.get(), Kg,
-                                                           chunks, rout, (uint32_t)wb);
-            DCX_CHECK_LAUNCH();
-            c.launched(2);
+            c.launched();
         };
         run_group(small, small_ids);
         run_group(big, big_ids);

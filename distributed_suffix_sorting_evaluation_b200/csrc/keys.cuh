@@ -217,16 +217,30 @@ constexpr size_t keys_slide_smem() {
 
 // Text id of every sorted element: the key is text-major and text s has
 // start[s+1] - start[s] elements, so it owns sorted slots [start[s], start[s+1]).
-// One binary search per thread, then a run of consecutive slots.
-__global__ void k_fill_segw(SegView sv, uint64_t N, uint32_t* __restrict__ segw) {
-    constexpr uint32_t RUN = 16;
-    for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * RUN; b < N;
-         b += (uint64_t)gridDim.x * blockDim.x * RUN) {
-        uint32_t s = seg_of(sv, b);
-        for (uint64_t k = b; k < b + RUN && k < N; k++) {
-            while (k >= sv.start[s + 1]) s++;
-            segw[k] = s;
+// A block covers FILL_TILE consecutive slots: two binary searches bound the
+// texts of the tile, and each slot searches only inside that range (zero steps
+// when the tile lies in one text); stores are coalesced.
+constexpr uint32_t FILL_TILE = 2048;
+
+__global__ __launch_bounds__(256) void k_fill_segw(SegView sv, uint64_t N, uint32_t* __restrict__ segw) {
+    __shared__ uint32_t s_lo, s_hi;
+    for (uint64_t t = (uint64_t)blockIdx.x * FILL_TILE; t < N; t += (uint64_t)gridDim.x * FILL_TILE) {
+        const uint64_t e = t + FILL_TILE < N ? t + FILL_TILE : N;
+        if (threadIdx.x == 0) {
+            s_lo = seg_of(sv, t);
+            s_hi = seg_of(sv, e - 1);
         }
+        __syncthreads();
+        const uint32_t lo0 = s_lo, hi0 = s_hi;
+        for (uint64_t k = t + threadIdx.x; k < e; k += blockDim.x) {
+            uint32_t lo = lo0, hi = hi0 + 1;  // largest s in [lo0, hi0] with start[s] <= k
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sv.start[mid] <= k) lo = mid; else hi = mid;
+            }
+            segw[k] = lo;
+        }
+        __syncthreads();
     }
 }
 

@@ -148,22 +148,6 @@ __global__ void k_spread_texts(const uint8_t* __restrict__ in, const uint64_t* _
     }
 }
 
-// Group outputs (goff layout, wb bytes per entry) to the texts' slots in the
-// round's output (src_off layout), by the same chunks as k_spread_texts.
-__global__ void k_scatter_outputs(const uint8_t* __restrict__ gout, const uint64_t* __restrict__ src_off,
-                                  const uint64_t* __restrict__ goff, const uint64_t* __restrict__ cbase, uint32_t K,
-                                  uint64_t chunks, uint8_t* __restrict__ out, uint32_t wb) {
-    for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-        const uint32_t k = chunk_text(cbase, K, c);
-        const uint64_t len = goff[k + 1] - goff[k];
-        const uint64_t lo = (c - cbase[k]) * TEXT_CHUNK;
-        const uint64_t hi = lo + TEXT_CHUNK < len ? lo + TEXT_CHUNK : len;
-        const uint8_t* src = gout + goff[k] * wb;
-        uint8_t* dst = out + src_off[k] * wb;
-        for (uint64_t i = lo * wb + threadIdx.x; i < hi * wb; i += blockDim.x) dst[i] = src[i];
-    }
-}
-
 // ---- head flags --------------------------------------------------------------
 struct KeyWords {
     const uint32_t* w[12];
@@ -591,18 +575,6 @@ __global__ void k_emit(const uint32_t* __restrict__ sa_full, uint64_t n, void* _
     }
 }
 
-__device__ __forceinline__ void store_sa_entry(void* out, uint64_t k, uint32_t v, int width) {
-    if (width == 32) reinterpret_cast<uint32_t*>(out)[k] = v;
-    else if (width == 64) reinterpret_cast<uint64_t*>(out)[k] = v;
-    else {
-        uint8_t* o = reinterpret_cast<uint8_t*>(out) + 5 * k;
-        o[0] = (uint8_t)v;
-        o[1] = (uint8_t)(v >> 8);
-        o[2] = (uint8_t)(v >> 16);
-        o[3] = (uint8_t)(v >> 24);
-        o[4] = 0;
-    }
-}
 
 // Several texts: sorted element k belongs to text s = segw[k]; text s's elements
 // occupy sorted slots [start[s], start[s+1]) with its empty suffix first, so
@@ -610,7 +582,7 @@ __device__ __forceinline__ void store_sa_entry(void* out, uint64_t k, uint32_t v
 __global__ void k_emit_seg(const uint32_t* __restrict__ sa_full, const uint32_t* __restrict__ segw, uint64_t N,
                            LevelSeg ls, void* __restrict__ out, int width) {
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < N; k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = segw[k];
+        const uint32_t s = segw ? segw[k] : 0u;  // no segw: a single text
         const uint64_t r = k - ls.start[s];
         if (r == 0) continue;
         store_sa_entry(out, ls.obase[s] + r - 1, (uint32_t)(sa_full[k] - ls.start[s]), width);

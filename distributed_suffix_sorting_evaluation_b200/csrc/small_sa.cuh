@@ -18,12 +18,13 @@ constexpr int SMALL_MAX = 2048;
 constexpr int SMALL_THREADS = 1024;
 
 // String s of the launch is text[start[s] .. start[s+1]-1) (each string is
-// followed by its 0); its SA (string-local indices) goes to out + obase[s].
+// followed by its 0); its SA (string-local indices) goes to entries [obase[s], obase[s] + n) of
+// out, `width` bits per entry.
 // Chars must be >= 1.
 template <typename CharT>
 __global__ __launch_bounds__(SMALL_THREADS) void k_small_sa(const CharT* __restrict__ text,
                                                             const uint64_t* __restrict__ start,
-                                                            const uint64_t* __restrict__ obase, uint32_t* __restrict__ out) {
+                                                            const uint64_t* __restrict__ obase, void* __restrict__ out, int width) {
     __shared__ uint64_t key[SMALL_MAX];
     __shared__ uint16_t idx[SMALL_MAX];
     __shared__ uint32_t rank[SMALL_MAX];
@@ -35,11 +36,11 @@ __global__ __launch_bounds__(SMALL_THREADS) void k_small_sa(const CharT* __restr
     const uint32_t n = (uint32_t)(start[s + 1] - b - 1);
     if (n == 0) return;
     const CharT* t = text + b;
-    out += obase[s];
+    const uint64_t ob = obase[s];
     for (uint32_t i = threadIdx.x; i < n; i += SMALL_THREADS) rank[i] = (uint32_t)t[i];
     __syncthreads();
     if (n == 1) {
-        if (threadIdx.x == 0) out[0] = 0;
+        if (threadIdx.x == 0) store_sa_entry(out, ob, 0u, width);
         return;
     }
     uint32_t C = 2;
@@ -95,7 +96,7 @@ __global__ __launch_bounds__(SMALL_THREADS) void k_small_sa(const CharT* __restr
         __syncthreads();
         if (s_done) break;
     }
-    for (uint32_t k = threadIdx.x; k < n; k += SMALL_THREADS) out[k] = idx[k];
+    for (uint32_t k = threadIdx.x; k < n; k += SMALL_THREADS) store_sa_entry(out, ob + k, idx[k], width);
 }
 
 }  // namespace dcx
