@@ -203,6 +203,47 @@ def run_reference_batch(args, world, rank):
     return 0
 
 
+def run_reference_serve(args, world, rank):
+    """Reference arm of the serving workload: libsais64_omp per request, in
+    arrival order, over the first requests up to --ref-sample-mib of text."""
+    if rank != 0:
+        return 0
+    from distributed_suffix_sorting_evaluation_b200 import workloads as W
+    from oracle import oracle as O
+    base_n = 1 << 30
+    lens = W.batch_lengths(args.serve_requests, 4 << 10, 256 << 20, seed=6).astype(np.int64)
+    rng = np.random.default_rng(7)
+    offs = (rng.random(lens.size) * (base_n - lens)).astype(np.int64)
+    base = W.markov_dna(base_n, seed=2)
+    threads = os.cpu_count() or 1
+    cap = args.ref_sample_mib << 20
+    k, tot = 0, 0
+    while k < lens.size and (k == 0 or tot + int(lens[k]) <= cap):
+        tot += int(lens[k])
+        k += 1
+    O.libsais(base[: 1 << 20], threads=threads)
+    vals = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        for i in range(k):
+            O.libsais(base[offs[i]:offs[i] + lens[i]], threads=threads)
+        vals.append(tot / GiB / (time.perf_counter() - t0))
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "served SA build GiB/s", "value": round(value, 4), "unit": "GiB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot / GiB / value * 1000, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "cfg5_serve", "lengths": "log-uniform 4 KiB-256 MiB", "sa_width": 32},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GiB/s", "cores": threads, "kind": "reference",
+                         "sample": f"libsais64_omp per request on the first {k} requests "
+                                   f"({tot >> 20} MiB), {threads} threads"},
+        "e2e": {"value": round(value, 4), "unit": "GiB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gpu(args, world, rank, local):
     import torch
     from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
@@ -462,6 +503,173 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+def run_serve(args, world, rank, local):
+    """Serving workload: SA requests with lengths log-uniform in [4 KiB, 256 MiB]
+    (seeded), each a distinct slice of a 1 GiB order-3 Markov DNA text (5%
+    repeats), DC39, 32-bit SA, under a 150 GB serving budget.
+      capacity  closed loop: the first requests (about --serve-cap-gib of text)
+                submitted back to back, time until the last is done;
+      served    open loop: Poisson arrivals at 80% of that capacity for
+                --serve-seconds; p50/p99 of submit -> done latency (SA complete
+                in HBM) and the sustained GiB/s of finished requests;
+      plain     the per-request path on the same requests: one dcx_build_sa per
+                request on its slice already in HBM (no upload), while
+                --loop-budget-s lasts.
+    Texts are uploaded by the server (pageable host copies) inside the latency."""
+    import torch
+    from distributed_suffix_sorting_evaluation_b200 import Context, SERVE_DONE, workloads as W
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
+    base_n = 1 << 30
+    base = W.markov_dna(base_n, seed=2 + 1000 * rank)
+    count = args.serve_requests
+    lens = W.batch_lengths(count, 4 << 10, 256 << 20, seed=6).astype(np.int64)
+    rng = np.random.default_rng(7 + rank)
+    offs = (rng.random(count) * (base_n - lens)).astype(np.int64)
+    ctx = Context(local)
+    ctx.set_option("serve_budget", args.serve_budget_gb * 1e9)
+    ctx.set_option("serve_lanes", args.serve_lanes)
+
+    def submit(i):
+        return ctx.serve_submit(None, dc=39, sa_width=32, text_ptr=base.ctypes.data + int(offs[i]), n=int(lens[i]))
+
+    # warm-up: a few requests of every size class through all lanes
+    wids = [submit(i) for i in range(min(count, 3 * args.serve_lanes))]
+    ctx.serve_drain()
+    for r in wids:
+        ctx.serve_release(r)
+
+    # 1. capacity (closed loop)
+    cap_bytes = args.serve_cap_gib << 30
+    k, tot = 0, 0
+    while k < count and tot < cap_bytes:
+        tot += int(lens[k])
+        k += 1
+    t0 = time.perf_counter()
+    ids = [submit(i) for i in range(k)]
+    ctx.serve_drain()
+    t_cap = time.perf_counter() - t0
+    for r in ids:
+        ctx.serve_release(r)
+    capacity = tot / GiB / t_cap
+
+    # 2. open loop: Poisson arrivals at 80% of capacity
+    mean_len = float(lens.mean())
+    rate = 0.8 * capacity * GiB / mean_len  # requests per second
+    arr = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    n_req = int(np.searchsorted(arr, args.serve_seconds))
+    n_req = max(1, min(n_req, count))
+    lat, last_done, failed = [], [0.0], []
+    nonlocal_done = [0]
+    pending = {}
+    lock = threading.Lock()
+    stop = threading.Event()
+
+    def poller():
+        while not (stop.is_set() and not pending):
+            with lock:
+                items = list(pending.items())
+            finished = []
+            for rid, n in items:
+                st, ms = ctx.serve_poll(rid)
+                if st < 0:
+                    failed.append(st)
+                if st == SERVE_DONE or st < 0:
+                    finished.append((rid, n, ms))
+            for rid, n, ms in finished:
+                ctx.serve_release(rid)
+                with lock:
+                    del pending[rid]
+                lat.append(ms)
+                nonlocal_done[0] += n
+                last_done[0] = time.perf_counter()
+            if not finished:
+                time.sleep(0.0002)
+
+    th = threading.Thread(target=poller)
+    with ClockSampler(local) as clocks:
+        start = time.perf_counter()
+        th.start()
+        for i in range(n_req):
+            wait = start + float(arr[i]) - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            rid = submit(i % count)
+            with lock:
+                pending[rid] = int(lens[i % count])
+        stop.set()
+        th.join()
+    clock = clocks.summary()
+    if failed:
+        raise SystemExit(f"{len(failed)} serving requests failed (first code {failed[0]})")
+    served_s = last_done[0] - start
+    done_bytes = nonlocal_done[0]
+    sustained = done_bytes / GiB / served_s
+    sstats = ctx.serve_stats()
+    lat_a = np.array(lat)
+
+    # 3. plain per-request path on the same requests, text already in HBM
+    d_base = torch.from_numpy(base).to(f"cuda:{local}")
+    d_sa = torch.empty(int(lens.max()) + 16, dtype=torch.int32, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    ctx.build_sa_device(d_base.data_ptr() + int(offs[0]), int(lens[0]), d_sa.data_ptr(), dc=39, sa_width=32)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    plain_ms, plain_bytes, j = 0.0, 0, 0
+    while j < n_req and plain_ms < args.loop_budget_s * 1000.0:
+        e0.record(stream)
+        ctx.build_sa_device(d_base.data_ptr() + int(offs[j]), int(lens[j]), d_sa.data_ptr(), dc=39, sa_width=32)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        plain_bytes += int(lens[j])
+        j += 1
+    plain = plain_bytes / GiB / (plain_ms / 1000.0)
+    # the served path on exactly those j requests, closed loop
+    t0 = time.perf_counter()
+    ids = [submit(i) for i in range(j)]
+    ctx.serve_drain()
+    same = plain_bytes / GiB / (time.perf_counter() - t0)
+    for r in ids:
+        ctx.serve_release(r)
+
+    if rank == 0:
+        line = {
+            "metric": "served SA build GiB/s", "value": round(sustained, 4), "unit": "GiB/s", "n_gpus": world,
+            "steps": n_req, "warmup": len(wids), "ms_per_step": round(served_s * 1000 / n_req, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (slices of a seeded 1 GiB order-3 Markov DNA text, 5% repeats)",
+            "config": {"workload": "cfg5_serve", "lengths": "log-uniform 4 KiB-256 MiB", "dc": 39, "sa_width": 32,
+                       "budget_gb": args.serve_budget_gb, "lanes": args.serve_lanes,
+                       "arrivals": "Poisson at 80% of measured capacity",
+                       "l2_flush": "batches up to 1 GiB of text, larger than L2",
+                       "parallelism": "replicas" if world > 1 else "single-gpu"},
+            "latency_ms": {"p50": round(float(np.percentile(lat_a, 50)), 2),
+                           "p99": round(float(np.percentile(lat_a, 99)), 2),
+                           "max": round(float(lat_a.max()), 2), "requests": int(lat_a.size),
+                           "definition": "submit -> SA complete in HBM, including queueing and upload"},
+            "offered": {"requests_per_s": round(rate, 2), "gib_per_s": round(0.8 * capacity, 4),
+                        "seconds": round(served_s, 2), "bytes": int(done_bytes)},
+            "capacity": {"value": round(capacity, 4), "unit": "GiB/s", "requests": k, "bytes": int(tot),
+                         "seconds": round(t_cap, 3)},
+            "plain": {"value": round(plain, 4), "unit": "GiB/s", "requests": j, "bytes": plain_bytes,
+                      "call": "dcx_build_sa per request, device pointers, text resident",
+                      "served_same_requests": round(same, 4), "speedup": round(same / plain, 3)},
+            "serve_stats": sstats,
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -478,8 +686,17 @@ def main():
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")
     ap.add_argument("--verify", action="store_true", help="check three SAs of every batched chunk on the GPU")
+    ap.add_argument("--serve-requests", type=int, default=20000, help="request pool of the serving workload")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="open-loop arrival window")
+    ap.add_argument("--serve-cap-gib", type=int, default=16, help="text of the closed-loop capacity run")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-lanes", type=int, default=3)
     args = ap.parse_args()
     world, rank, local = _dist()
+    if args.workload == "cfg5_serve":
+        if args.impl == "reference":
+            return run_reference_serve(args, world, rank)
+        return run_serve(args, world, rank, local)
     if args.workload == "cfg4_batch":
         if args.impl == "reference":
             return run_reference_batch(args, world, rank)

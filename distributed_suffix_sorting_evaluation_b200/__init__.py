@@ -48,8 +48,11 @@ EXPORTED = (
     "dcx_ctx_create", "dcx_ctx_destroy", "dcx_set_option", "dcx_build_sa", "dcx_build_sa_strict",
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
-    "dcx_build_sa_noalloc", "dcx_check_sa",
+    "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
 )
+
+# serving request states (dcx_serve_poll)
+SERVE_QUEUED, SERVE_RUNNING, SERVE_DONE = 0, 1, 2
 
 
 class DcxError(RuntimeError):
@@ -68,6 +71,19 @@ class DcxStats(ctypes.Structure):
         ("sigma", ctypes.c_uint32), ("level0_samples", ctypes.c_uint64), ("level0_last_rank", ctypes.c_uint64),
         ("level0_recursion", ctypes.c_int), ("level0_reduction", ctypes.c_double),
         ("tie_groups", ctypes.c_uint64), ("tie_elements", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [
+        ("lanes", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64), ("reserved_bytes", ctypes.c_uint64),
+        ("peak_reserved_bytes", ctypes.c_uint64), ("peak_lane_bytes", ctypes.c_uint64),
+        ("submitted", ctypes.c_uint64), ("done", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+        ("done_bytes", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("max_batch_texts", ctypes.c_uint64),
+        ("queued", ctypes.c_uint64), ("running_batches", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -101,6 +117,8 @@ def load_library(path: str | None = None):
     lib.dcx_serve_poll.argtypes = [vp, u64, vp, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]
     lib.dcx_serve_release.argtypes = [vp, u64]
     lib.dcx_serve_drain.argtypes = [vp]
+    lib.dcx_serve_result_device.argtypes = [vp, u64, ctypes.POINTER(vp)]
+    lib.dcx_serve_get_stats.argtypes = [vp, ctypes.POINTER(ServeStats)]
     lib.dcx_strerror.argtypes = [i32]
     lib.dcx_strerror.restype = ctypes.c_char_p
     lib.dcx_dc_table.argtypes = [i32, vp, vp, vp, vp]
@@ -231,6 +249,13 @@ class Context:
                                      ctypes.byref(ok)))
         return bool(ok.value)
 
+    def check_sa_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int) -> bool:
+        """GPU check of a device-resident SA against a device-resident text."""
+        ok = ctypes.c_int()
+        _check(self.lib.dcx_check_sa(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
+                                     DCX_DEVICE_PTRS, ctypes.byref(ok)))
+        return bool(ok.value)
+
     def stream_handle(self) -> int:
         """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""
         p = ctypes.c_void_p()
@@ -248,6 +273,57 @@ class Context:
         s = DcxStats()
         _check(self.lib.dcx_get_stats(self.h, ctypes.byref(s)))
         return s.as_dict()
+
+    # ---- serving -------------------------------------------------------------
+    def serve_submit(self, text, dc: int = 0, sa_width: int = 32, text_ptr: int | None = None,
+                     n: int | None = None) -> int:
+        """Queues an SA request (the text is copied); returns its id.  Pass either
+        `text` (bytes / uint8 array) or a raw host pointer and length."""
+        if text_ptr is None:
+            t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                     else np.asarray(text, dtype=np.uint8))
+            text_ptr, n = (t.ctypes.data if t.size else None), t.size
+        rid = ctypes.c_uint64()
+        _check(self.lib.dcx_serve_submit(self.h, ctypes.c_void_p(text_ptr) if text_ptr else None, n, dc, sa_width,
+                                         ctypes.byref(rid)))
+        return rid.value
+
+    def serve_poll(self, rid: int, out: np.ndarray | None = None):
+        """(status, latency_ms); when done and `out` (uint8, n * sa_width/8 bytes)
+        is given, the SA is copied into it."""
+        st = ctypes.c_int()
+        lat = ctypes.c_double()
+        _check(self.lib.dcx_serve_poll(self.h, rid, out.ctypes.data if out is not None and out.size else None,
+                                       ctypes.byref(st), ctypes.byref(lat)))
+        return st.value, lat.value
+
+    def serve_result_device(self, rid: int) -> int:
+        p = ctypes.c_void_p()
+        _check(self.lib.dcx_serve_result_device(self.h, rid, ctypes.byref(p)))
+        return p.value or 0
+
+    def serve_release(self, rid: int):
+        _check(self.lib.dcx_serve_release(self.h, rid))
+
+    def serve_drain(self):
+        _check(self.lib.dcx_serve_drain(self.h))
+
+    def serve_stats(self) -> dict:
+        s = ServeStats()
+        _check(self.lib.dcx_serve_get_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def serve_result(self, rid: int, n: int, sa_width: int = 32) -> np.ndarray:
+        """Waits for request `rid` (n chars) and returns its SA as uint64."""
+        import time
+        out = np.zeros(max(n, 1) * sa_dtype_bytes(sa_width), np.uint8)
+        while True:
+            st, _ = self.serve_poll(rid, out)
+            if st == SERVE_DONE:
+                return unpack_sa(out, sa_width, n)
+            if st < 0:
+                raise DcxError(st, "serving request failed")
+            time.sleep(0.0005)
 
     def trace(self):
         """Level-0 names and unique flags of the last build with option trace=1."""

@@ -201,6 +201,11 @@ struct Options {
     int trace = 0;
     uint32_t spin_limit = 1u << 24;
     uint64_t batch_round_cap = 0;  // max elements per batch round (0 = from the budget)
+    // serving
+    uint32_t serve_lanes = 3;
+    uint64_t serve_budget = 0;  // 0 = the context budget
+    uint64_t serve_batch_bytes = 1ull << 30;
+    uint32_t serve_batch_texts = 65536;
 };
 
 struct Ctx;
@@ -1400,11 +1405,59 @@ static bool check_one(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
 
 }  // namespace dcx
 
+#include "serve.cuh"
+
+namespace dcx {
+
+static void ctx_init(Ctx& c, int device, uint64_t budget) {
+    c.device = device;
+    DCX_CUDA(cudaSetDevice(device));
+    DCX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    cudaMemPool_t pool;
+    DCX_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    DCX_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    size_t fr = 0, tot = 0;
+    DCX_CUDA(cudaMemGetInfo(&fr, &tot));
+    c.budget = budget ? budget : (uint64_t)(fr * 0.9);
+    DCX_CUDA(cudaMalloc(&c.d_hist, 16 * RADIX * 4));
+    DCX_CUDA(cudaMalloc(&c.d_base, 16 * RADIX * 4));
+    DCX_CUDA(cudaMalloc(&c.d_tiles, 64 * 4));
+    DCX_CUDA(cudaMalloc(&c.d_err, 4));
+    DCX_CUDA(cudaMemset(c.d_err, 0, 4));
+    DCX_CUDA(cudaMalloc(&c.d_h256, 256 * 8));
+    DCX_CUDA(cudaHostAlloc((void**)&c.h_pinned, PINNED_WORDS * 4, cudaHostAllocDefault));
+}
+
+static void ctx_free(Ctx& c) {
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    cudaFree(c.d_hist);
+    cudaFree(c.d_base);
+    cudaFree(c.d_tiles);
+    cudaFree(c.d_err);
+    cudaFree(c.d_h256);
+    if (c.d_lookback) cudaFree(c.d_lookback);
+    if (c.h_pinned) cudaFreeHost(c.h_pinned);
+    for (auto& kv : c.dc_dev) cudaFree(kv.second);
+    for (auto& kv : c.dc_flags_dev) cudaFree(kv.second);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    c.stream = nullptr;
+    c.d_lookback = nullptr;
+    c.h_pinned = nullptr;
+    c.dc_dev.clear();
+    c.dc_flags_dev.clear();
+}
+
+}  // namespace dcx
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
 struct dcx_ctx {
     dcx::Ctx c;
+    std::mutex serve_mu;
+    std::unique_ptr<dcx::Server> server;  // started by the first dcx_serve_submit
 };
 
 using dcx::Error;
@@ -1459,26 +1512,10 @@ int dcx_ctx_create(dcx_ctx** out, int device, uint64_t budget) {
     *out = nullptr;
     return guarded([&] {
         auto* x = new dcx_ctx();
-        dcx::Ctx& c = x->c;
         try {
-            c.device = device;
-            DCX_CUDA(cudaSetDevice(device));
-            DCX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-            cudaMemPool_t pool;
-            DCX_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-            uint64_t thr = UINT64_MAX;
-            DCX_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-            size_t fr = 0, tot = 0;
-            DCX_CUDA(cudaMemGetInfo(&fr, &tot));
-            c.budget = budget ? budget : (uint64_t)(fr * 0.9);
-            DCX_CUDA(cudaMalloc(&c.d_hist, 16 * dcx::RADIX * 4));
-            DCX_CUDA(cudaMalloc(&c.d_base, 16 * dcx::RADIX * 4));
-            DCX_CUDA(cudaMalloc(&c.d_tiles, 64 * 4));
-            DCX_CUDA(cudaMalloc(&c.d_err, 4));
-            DCX_CUDA(cudaMemset(c.d_err, 0, 4));
-            DCX_CUDA(cudaMalloc(&c.d_h256, 256 * 8));
-            DCX_CUDA(cudaHostAlloc((void**)&c.h_pinned, dcx::PINNED_WORDS * 4, cudaHostAllocDefault));
+            dcx::ctx_init(x->c, device, budget);
         } catch (...) {
+            dcx::ctx_free(x->c);
             delete x;
             throw;
         }
@@ -1489,18 +1526,8 @@ int dcx_ctx_create(dcx_ctx** out, int device, uint64_t budget) {
 int dcx_ctx_destroy(dcx_ctx* x) {
     if (!x) return DCX_ERR_ARG;
     return guarded([&] {
-        dcx::Ctx& c = x->c;
-        cudaSetDevice(c.device);
-        if (c.stream) cudaStreamSynchronize(c.stream);
-        cudaFree(c.d_hist);
-        cudaFree(c.d_base);
-        cudaFree(c.d_tiles);
-        cudaFree(c.d_err);
-        cudaFree(c.d_h256);
-        if (c.d_lookback) cudaFree(c.d_lookback);
-        if (c.h_pinned) cudaFreeHost(c.h_pinned);
-        for (auto& kv : c.dc_dev) cudaFree(kv.second);
-        if (c.stream) cudaStreamDestroy(c.stream);
+        x->server.reset();  // joins the lanes, frees unreleased results
+        dcx::ctx_free(x->c);
         delete x;
     });
 }
@@ -1521,7 +1548,17 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
     else if (s == "trace") o.trace = value != 0;
     else if (s == "spin_limit") o.spin_limit = (uint32_t)value;
     else if (s == "batch_round_cap") o.batch_round_cap = (uint64_t)value;
-    else return DCX_ERR_ARG;
+    else if (s == "serve_lanes") {
+        if (value < 1 || value > 16) return DCX_ERR_ARG;
+        o.serve_lanes = (uint32_t)value;
+    } else if (s == "serve_budget") o.serve_budget = (uint64_t)value;
+    else if (s == "serve_batch_bytes") {
+        if (value < 1) return DCX_ERR_ARG;
+        o.serve_batch_bytes = (uint64_t)value;
+    } else if (s == "serve_batch_texts") {
+        if (value < 1) return DCX_ERR_ARG;
+        o.serve_batch_texts = (uint32_t)value;
+    } else return DCX_ERR_ARG;
     return DCX_OK;
 }
 
@@ -1586,9 +1623,55 @@ int dcx_build_sa_batch(dcx_ctx* x, const uint8_t* texts, const uint64_t* offsets
         dcx::build_batch(x->c, texts, offsets, num_texts, dc_or_auto, sa_width, sa_out, flags);
     });
 }
-int dcx_serve_submit(dcx_ctx*, const uint8_t*, uint64_t, int, int, uint64_t*) { return DCX_ERR_INTERNAL; }
-int dcx_serve_poll(dcx_ctx*, uint64_t, void*, int*, double*) { return DCX_ERR_INTERNAL; }
-int dcx_serve_release(dcx_ctx*, uint64_t) { return DCX_ERR_INTERNAL; }
-int dcx_serve_drain(dcx_ctx*) { return DCX_OK; }
+static dcx::Server& server_of(dcx_ctx* x) {
+    std::lock_guard<std::mutex> lk(x->serve_mu);
+    if (!x->server) {
+        const dcx::Options& o = x->c.opt;
+        const uint64_t budget = o.serve_budget ? o.serve_budget : x->c.budget;
+        x->server = std::make_unique<dcx::Server>(x->c, (int)o.serve_lanes, budget, o.serve_batch_bytes,
+                                                  o.serve_batch_texts);
+    }
+    return *x->server;
+}
+
+int dcx_serve_submit(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int sa_width, uint64_t* req_id) {
+    if (!x || !req_id) return DCX_ERR_ARG;
+    return guarded([&] { *req_id = server_of(x).submit(text, n, dc, sa_width); });
+}
+
+int dcx_serve_poll(dcx_ctx* x, uint64_t req_id, void* sa_host, int* status, double* latency_ms) {
+    if (!x || !status) return DCX_ERR_ARG;
+    return guarded([&] { server_of(x).poll(req_id, sa_host, status, latency_ms); });
+}
+
+int dcx_serve_result_device(dcx_ctx* x, uint64_t req_id, const void** sa_dev) {
+    if (!x || !sa_dev) return DCX_ERR_ARG;
+    return guarded([&] { *sa_dev = server_of(x).result_device(req_id); });
+}
+
+int dcx_serve_release(dcx_ctx* x, uint64_t req_id) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] { server_of(x).release(req_id); });
+}
+
+int dcx_serve_drain(dcx_ctx* x) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        dcx::Server* sv;
+        {
+            std::lock_guard<std::mutex> lk(x->serve_mu);
+            sv = x->server.get();
+        }
+        if (sv) sv->drain();
+    });
+}
+
+int dcx_serve_get_stats(dcx_ctx* x, dcx_serve_stats* out) {
+    if (!x || !out) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->serve_mu);
+        *out = x->server ? x->server->stats() : dcx_serve_stats{};
+    });
+}
 
 }  // extern "C"

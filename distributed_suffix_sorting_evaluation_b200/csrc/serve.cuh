@@ -1,0 +1,335 @@
+// Serving: continuous batching of SA requests on one GPU.
+//
+// The reference builds one SA per process run (cli.cpp:747-820); it has no
+// request loop.  This server keeps the DCX pipeline of build_batch as its unit
+// of work and adds what a long-running service needs:
+//   * requests are copied at submission and queued in arrival order;
+//   * L lanes (threads, each with its own stream and scratch context) take
+//     work whenever they are free, so requests arriving while other batches
+//     run start at once on a free lane and overlap with them on the device;
+//   * a lane admits the queued requests of one (dc, sa_width) class, first come
+//     first served, while their projected footprint fits the HBM budget and the
+//     batch stays under a text-byte cap; a request that does not fit waits for
+//     memory to be released (results count until dcx_serve_release);
+//   * results stay on the device until the caller polls (copy to host) and
+//     releases them.
+// Every result is the SA build_batch computes for that text alone, because a
+// text's SA does not depend on the other texts of its batch (the text id is
+// the most significant key digit and every per-text quantity is segment-local).
+#pragma once
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace dcx {
+
+// Device bytes a request may hold while its batch runs: the build scratch
+// (build_batch plans 48 bytes per element), the device copy of the text and
+// the result.  The result part stays reserved until the request is released.
+static uint64_t serve_scratch_bytes(uint64_t n) { return 48 * (n + 1) + (1ull << 20); }
+static uint64_t serve_result_bytes(uint64_t n, int width) { return ((n * (uint64_t)(width / 8)) + 16 + 255) & ~255ull; }
+static uint64_t serve_footprint(uint64_t n, int width) {
+    return serve_scratch_bytes(n) + ((n + 16 + 255) & ~255ull) + serve_result_bytes(n, width);
+}
+
+static void ctx_init(Ctx& c, int device, uint64_t budget);
+static void ctx_free(Ctx& c);
+
+// A batch's result buffer, shared by its requests; freed with the last of them.
+struct ServeResult {
+    void* p = nullptr;
+    uint64_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t refs = 0;  // requests not yet released (guarded by the server mutex)
+    ~ServeResult() {
+        if (p) cudaFreeAsync(p, stream);
+    }
+};
+
+struct ServeReq {
+    uint64_t id = 0;
+    std::vector<uint8_t> text;  // host copy until the batch has uploaded it
+    uint64_t n = 0;
+    int dc = 0, width = 32;
+    uint64_t footprint = 0;
+    int status = 0;  // 0 queued, 1 running, 2 done, < 0 failed (error code)
+    int lane = -1;
+    std::chrono::steady_clock::time_point t_submit, t_start, t_done;
+    std::shared_ptr<ServeResult> res;
+    uint64_t res_off = 0;  // byte offset of this request's SA in res
+};
+
+class Server {
+public:
+    Server(const Ctx& parent, int lanes, uint64_t budget, uint64_t batch_bytes, uint32_t batch_texts)
+        : device_(parent.device), budget_(budget), batch_bytes_(batch_bytes), batch_texts_(batch_texts) {
+        st_.lanes = (uint32_t)lanes;
+        st_.budget_bytes = budget;
+        for (int k = 0; k < lanes; k++) {
+            auto c = std::make_unique<Ctx>();
+            ctx_init(*c, device_, 0);
+            c->opt = parent.opt;
+            c->opt.trace = 0;
+            lanes_.push_back(std::move(c));
+        }
+        DCX_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+        for (int k = 0; k < lanes; k++) threads_.emplace_back([this, k] { lane_main(k); });
+    }
+
+    ~Server() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_work_.notify_all();
+        for (auto& t : threads_) t.join();
+        reqs_.clear();  // frees the results on their lanes' streams
+        for (auto& c : lanes_) {
+            cudaStreamSynchronize(c->stream);
+            ctx_free(*c);
+        }
+        cudaStreamDestroy(copy_stream_);
+    }
+
+    uint64_t submit(const uint8_t* text, uint64_t n, int dc, int width) {
+        if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+        if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+        if (n && !text) throw Error(DCX_ERR_ARG, "null pointer");
+        if (dc != 0) {
+            DcHost h;
+            if (!make_dc((uint32_t)dc, h)) throw Error(DCX_ERR_ARG, "unsupported difference cover");
+        }
+        const uint64_t fp = serve_footprint(n, width);
+        if (fp > budget_) throw Error(DCX_ERR_BUDGET, "request footprint above the serving budget");
+        auto r = std::make_unique<ServeReq>();
+        r->text.assign(text, text + n);
+        r->n = n;
+        r->dc = dc;
+        r->width = width;
+        r->footprint = fp;
+        r->t_submit = std::chrono::steady_clock::now();
+        uint64_t id;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (stop_) throw Error(DCX_ERR_INTERNAL, "server stopped");
+            id = next_id_++;
+            r->id = id;
+            queue_.push_back(id);
+            reqs_[id] = std::move(r);
+            st_.submitted++;
+        }
+        cv_work_.notify_one();
+        return id;
+    }
+
+    // status / latency; copies the SA to sa_host when done and sa_host != null
+    void poll(uint64_t id, void* sa_host, int* status, double* latency_ms) {
+        std::shared_ptr<ServeResult> res;
+        uint64_t off = 0, bytes = 0;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            auto it = reqs_.find(id);
+            if (it == reqs_.end()) throw Error(DCX_ERR_NOTFOUND, "unknown or released request");
+            ServeReq& r = *it->second;
+            if (status) *status = r.status;
+            if (latency_ms)
+                *latency_ms = r.status == 2 ? std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count()
+                                            : 0.0;
+            if (r.status != 2 || !sa_host) return;
+            res = r.res;
+            off = r.res_off;
+            bytes = r.n * (uint64_t)(r.width / 8);
+        }
+        if (bytes) {
+            std::lock_guard<std::mutex> lk(copy_mu_);
+            DCX_CUDA(cudaSetDevice(device_));
+            DCX_CUDA(cudaMemcpyAsync(sa_host, (const uint8_t*)res->p + off, bytes, cudaMemcpyDeviceToHost, copy_stream_));
+            DCX_CUDA(cudaStreamSynchronize(copy_stream_));
+        }
+    }
+
+    const void* result_device(uint64_t id) {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = reqs_.find(id);
+        if (it == reqs_.end()) throw Error(DCX_ERR_NOTFOUND, "unknown or released request");
+        if (it->second->status != 2) throw Error(DCX_ERR_BUSY, "request not done");
+        if (!it->second->res) return nullptr;
+        return (const uint8_t*)it->second->res->p + it->second->res_off;
+    }
+
+    void release(uint64_t id) {
+        std::shared_ptr<ServeResult> drop;  // freed outside the lock
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            auto it = reqs_.find(id);
+            if (it == reqs_.end()) throw Error(DCX_ERR_NOTFOUND, "unknown or released request");
+            ServeReq& r = *it->second;
+            if (r.status == 0 || r.status == 1) throw Error(DCX_ERR_BUSY, "request still queued or running");
+            if (r.res && --r.res->refs == 0) {
+                reserved_ -= r.res->bytes;
+                drop = r.res;
+            }
+            reqs_.erase(it);
+        }
+        cv_work_.notify_all();
+    }
+
+    void drain() {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return queue_.empty() && running_ == 0; });
+    }
+
+    dcx_serve_stats stats() {
+        std::lock_guard<std::mutex> lk(mu_);
+        dcx_serve_stats s = st_;
+        s.reserved_bytes = reserved_;
+        s.queued = queue_.size();
+        s.running_batches = running_;
+        return s;
+    }
+
+private:
+    bool head_fits() const {
+        if (queue_.empty()) return false;
+        const ServeReq& r = *reqs_.at(queue_.front());
+        return reserved_ + r.footprint <= budget_;
+    }
+
+    void lane_main(int k) {
+        cudaSetDevice(device_);
+        Ctx& c = *lanes_[k];
+        for (;;) {
+            std::vector<ServeReq*> batch;
+            uint64_t scratch = 0, text_bytes = 0;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_work_.wait(lk, [&] { return stop_ || head_fits(); });
+                if (stop_) return;
+                const ServeReq& head = *reqs_.at(queue_.front());
+                const int dc = head.dc, width = head.width;
+                for (auto it = queue_.begin(); it != queue_.end();) {
+                    ServeReq* r = reqs_.at(*it).get();
+                    if (r->dc != dc || r->width != width) {  // another class: left for the next lane
+                        ++it;
+                        continue;
+                    }
+                    if (!batch.empty() &&
+                        (text_bytes + r->n > batch_bytes_ || batch.size() >= batch_texts_))
+                        break;
+                    if (reserved_ + r->footprint > budget_) break;  // first come, first served
+                    reserved_ += r->footprint;
+                    scratch += r->footprint - serve_result_bytes(r->n, width);
+                    text_bytes += r->n;
+                    r->status = 1;
+                    r->lane = k;
+                    r->t_start = std::chrono::steady_clock::now();
+                    batch.push_back(r);
+                    it = queue_.erase(it);
+                }
+                running_++;
+                st_.batches++;
+                st_.peak_reserved_bytes = std::max<uint64_t>(st_.peak_reserved_bytes, reserved_);
+                st_.max_batch_texts = std::max<uint64_t>(st_.max_batch_texts, batch.size());
+            }
+            cv_work_.notify_all();  // the rest of the queue may fit another lane
+            int err = DCX_OK;
+            std::shared_ptr<ServeResult> res;
+            std::vector<uint64_t> offs(batch.size() + 1, 0);
+            try {
+                res = run(c, batch, scratch, offs);
+            } catch (const Error& e) {
+                err = e.code;
+            } catch (...) {
+                err = DCX_ERR_INTERNAL;
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                const auto now = std::chrono::steady_clock::now();
+                uint64_t result_bytes = 0;
+                for (size_t i = 0; i < batch.size(); i++) {
+                    ServeReq* r = batch[i];
+                    r->t_done = now;
+                    std::vector<uint8_t>().swap(r->text);
+                    if (err == DCX_OK) {
+                        r->status = 2;
+                        r->res = res;
+                        r->res_off = offs[i] * (uint64_t)(r->width / 8);
+                        st_.done++;
+                        st_.done_bytes += r->n;
+                    } else {
+                        r->status = err;
+                        st_.failed++;
+                    }
+                }
+                if (err == DCX_OK && res) {
+                    res->refs = (uint32_t)batch.size();
+                    result_bytes = res->bytes;
+                }
+                // the scratch and text parts end with the batch, the result stays until released
+                uint64_t fp = 0;
+                for (ServeReq* r : batch) fp += r->footprint;
+                reserved_ -= fp - result_bytes;
+                st_.peak_lane_bytes = std::max<uint64_t>(st_.peak_lane_bytes, c.peak);
+                running_--;
+            }
+            cv_work_.notify_all();
+            cv_done_.notify_all();
+        }
+    }
+
+    // Uploads the batch's texts, builds their SAs into one device buffer.
+    std::shared_ptr<ServeResult> run(Ctx& c, const std::vector<ServeReq*>& batch, uint64_t scratch,
+                                     std::vector<uint64_t>& offs) {
+        const int width = batch[0]->width, dc = batch[0]->dc;
+        for (size_t i = 0; i < batch.size(); i++) offs[i + 1] = offs[i] + batch[i]->n;
+        const uint64_t total = offs.back();
+        auto res = std::make_shared<ServeResult>();
+        res->stream = c.stream;
+        res->bytes = serve_result_bytes(total, width);
+        void* d_text = nullptr;
+        DCX_CUDA(cudaMallocAsync(&d_text, total + 16, c.stream));
+        if (cudaMallocAsync(&res->p, res->bytes, c.stream) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeAsync(d_text, c.stream);
+            throw Error(DCX_ERR_OOM, "result buffer");
+        }
+        try {
+            for (size_t i = 0; i < batch.size(); i++)
+                if (batch[i]->n)
+                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)d_text + offs[i], batch[i]->text.data(), batch[i]->n,
+                                             cudaMemcpyHostToDevice, c.stream));
+            c.budget = c.in_use + scratch;  // build_batch sizes its rounds from this
+            build_batch(c, (const uint8_t*)d_text, offs.data(), (uint32_t)batch.size(), dc, width, res->p,
+                        DCX_DEVICE_PTRS);
+            DCX_CUDA(cudaStreamSynchronize(c.stream));
+        } catch (...) {
+            cudaFreeAsync(d_text, c.stream);
+            throw;
+        }
+        DCX_CUDA(cudaFreeAsync(d_text, c.stream));
+        return res;
+    }
+
+    int device_;
+    uint64_t budget_, batch_bytes_;
+    uint32_t batch_texts_;
+    std::mutex mu_, copy_mu_;
+    std::condition_variable cv_work_, cv_done_;
+    std::deque<uint64_t> queue_;
+    std::map<uint64_t, std::unique_ptr<ServeReq>> reqs_;
+    uint64_t next_id_ = 1, reserved_ = 0;
+    uint32_t running_ = 0;
+    bool stop_ = false;
+    dcx_serve_stats st_{};
+    std::vector<std::unique_ptr<Ctx>> lanes_;
+    std::vector<std::thread> threads_;
+    cudaStream_t copy_stream_ = nullptr;
+};
+
+}  // namespace dcx

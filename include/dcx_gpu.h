@@ -136,19 +136,51 @@ int dcx_build_sa_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offse
                        uint32_t flags);
 
 /* ---- serving (continuous batching) ----------------------------------------- */
-/* Admits an SA request.  The text is copied at submission; the request is
- * admitted to the GPU when its projected footprint fits the budget.  Returns
- * DCX_ERR_BUDGET if the request can never fit. */
+/* No counterpart in the reference (its cli builds one SA per run,
+ * cli.cpp:747-820).  A request loop on the context's GPU: requests are copied
+ * at submission and queued in arrival order; `serve_lanes` worker lanes (each
+ * its own stream) take the queued requests of one (dc, sa_width) class, first
+ * come first served, while their projected HBM footprint fits the serving
+ * budget, and build them as one batch (dcx_build_sa_batch semantics).  A lane
+ * that finishes takes whatever has arrived meanwhile, so new requests overlap
+ * on the device with the batches of the other lanes.  Results stay on the
+ * device (and count against the budget) until released.  Every result equals
+ * the SA of its text built alone.  All dcx_serve_* calls are thread-safe. */
+typedef struct dcx_serve_stats {
+    uint32_t lanes;
+    uint64_t budget_bytes;        /* serving HBM budget */
+    uint64_t reserved_bytes;      /* projected bytes of running batches + unreleased results */
+    uint64_t peak_reserved_bytes; /* high-water mark of reserved_bytes */
+    uint64_t peak_lane_bytes;     /* largest scratch high-water mark a lane measured in one batch */
+    uint64_t submitted, done, failed;
+    uint64_t done_bytes;          /* text bytes of finished requests */
+    uint64_t batches;             /* batches started */
+    uint64_t max_batch_texts;     /* most requests in one batch */
+    uint64_t queued;              /* requests waiting now */
+    uint32_t running_batches;     /* batches on the GPU now */
+} dcx_serve_stats;
+
+/* Queues an SA request (dc = 0: DC39; sa_width 32, 40 or 64).  Returns
+ * DCX_ERR_BUDGET if its projected footprint can never fit the budget.  The
+ * serving budget is the option "serve_budget" (bytes; 0 = the context budget),
+ * read when the first request starts the server, as are "serve_lanes"
+ * (default 3), "serve_batch_bytes" (text bytes per batch, default 1 GiB) and
+ * "serve_batch_texts" (requests per batch, default 65536). */
 int dcx_serve_submit(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
                      uint64_t* req_id);
 /* Polls a request: *status = 0 queued, 1 running, 2 done, <0 failed (error code).
  * When done and sa_host is non-null, copies the SA (n entries of sa_width bits)
- * into sa_host.  latency_ms (optional) receives submit->done wall time. */
+ * into sa_host.  latency_ms (optional) receives the submit -> done time (done =
+ * SA complete in device memory). */
 int dcx_serve_poll(dcx_ctx* ctx, uint64_t req_id, void* sa_host, int* status, double* latency_ms);
-/* Frees a finished request's result. */
+/* Device address of a finished request's SA (valid until released). */
+int dcx_serve_result_device(dcx_ctx* ctx, uint64_t req_id, const void** sa_dev);
+/* Frees a finished (or failed) request and its result; DCX_ERR_BUSY while it
+ * is queued or running, DCX_ERR_NOTFOUND for unknown ids. */
 int dcx_serve_release(dcx_ctx* ctx, uint64_t req_id);
-/* Blocks until every submitted request is done. */
+/* Blocks until no request is queued or running. */
 int dcx_serve_drain(dcx_ctx* ctx);
+int dcx_serve_get_stats(dcx_ctx* ctx, dcx_serve_stats* out);
 
 /* ---- allocation-free entry point ----------------------------------------- */
 /* No counterpart in the reference.  Suffix array of a device-resident text of
