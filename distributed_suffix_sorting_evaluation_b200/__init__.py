@@ -84,6 +84,7 @@ class ServeStats(ctypes.Structure):
         ("submitted", ctypes.c_uint64), ("done", ctypes.c_uint64), ("failed", ctypes.c_uint64),
         ("done_bytes", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("max_batch_texts", ctypes.c_uint64),
         ("queued", ctypes.c_uint64), ("running_batches", ctypes.c_uint32),
+        ("ms_upload", ctypes.c_double), ("ms_build", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:

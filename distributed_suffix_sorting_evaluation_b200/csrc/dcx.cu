@@ -206,6 +206,7 @@ struct Options {
     uint64_t serve_budget = 0;  // 0 = the context budget
     uint64_t serve_batch_bytes = 1ull << 30;
     uint32_t serve_batch_texts = 65536;
+    uint64_t serve_host_bytes = 8ull << 30;  // pinned host arena for request copies
 };
 
 struct Ctx;
@@ -1552,6 +1553,7 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
         if (value < 1 || value > 16) return DCX_ERR_ARG;
         o.serve_lanes = (uint32_t)value;
     } else if (s == "serve_budget") o.serve_budget = (uint64_t)value;
+    else if (s == "serve_host_bytes") o.serve_host_bytes = (uint64_t)value;
     else if (s == "serve_batch_bytes") {
         if (value < 1) return DCX_ERR_ARG;
         o.serve_batch_bytes = (uint64_t)value;
@@ -1629,7 +1631,7 @@ static dcx::Server& server_of(dcx_ctx* x) {
         const dcx::Options& o = x->c.opt;
         const uint64_t budget = o.serve_budget ? o.serve_budget : x->c.budget;
         x->server = std::make_unique<dcx::Server>(x->c, (int)o.serve_lanes, budget, o.serve_batch_bytes,
-                                                  o.serve_batch_texts);
+                                                  o.serve_batch_texts, o.serve_host_bytes);
     }
     return *x->server;
 }

@@ -41,6 +41,84 @@ static uint64_t serve_footprint(uint64_t n, int width) {
 static void ctx_init(Ctx& c, int device, uint64_t budget);
 static void ctx_free(Ctx& c);
 
+// Pinned host arena for the request copies, so a lane's upload is a DMA at
+// link speed rather than a staged pageable copy.  First fit over a free list
+// with coalescing; a request that does not fit falls back to pageable memory.
+class PinnedArena {
+public:
+    explicit PinnedArena(uint64_t bytes) {
+        if (bytes && cudaHostAlloc((void**)&base_, bytes, cudaHostAllocDefault) == cudaSuccess) {
+            size_ = bytes;
+            free_[0] = bytes;
+        } else {
+            cudaGetLastError();
+            base_ = nullptr;
+        }
+    }
+    ~PinnedArena() {
+        if (base_) cudaFreeHost(base_);
+    }
+    uint8_t* alloc(uint64_t n) {
+        n = (std::max<uint64_t>(n, 1) + 255) & ~255ull;
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            const uint64_t off = it->first, sz = it->second;
+            free_.erase(it);
+            if (sz > n) free_[off + n] = sz - n;
+            used_[off] = n;
+            return base_ + off;
+        }
+        return nullptr;
+    }
+    bool owns(const uint8_t* p) const { return base_ && p >= base_ && p < base_ + size_; }
+    void free(const uint8_t* p) {
+        std::lock_guard<std::mutex> lk(mu_);
+        const uint64_t off = (uint64_t)(p - base_);
+        auto u = used_.find(off);
+        if (u == used_.end()) return;
+        uint64_t o = off, sz = u->second;
+        used_.erase(u);
+        auto nx = free_.lower_bound(o);
+        if (nx != free_.end() && nx->first == o + sz) {  // merge with the next free block
+            sz += nx->second;
+            nx = free_.erase(nx);
+        }
+        if (nx != free_.begin()) {  // merge with the previous free block
+            auto pv = std::prev(nx);
+            if (pv->first + pv->second == o) {
+                pv->second += sz;
+                return;
+            }
+        }
+        free_[o] = sz;
+    }
+
+private:
+    uint8_t* base_ = nullptr;
+    uint64_t size_ = 0;
+    std::mutex mu_;
+    std::map<uint64_t, uint64_t> free_, used_;
+};
+
+// Host copy of a request text: large texts are split over a few threads, since
+// one core's memcpy would bound the submission rate well below the GPU's.
+static void parallel_copy(uint8_t* dst, const uint8_t* src, uint64_t n) {
+    constexpr uint64_t PIECE = 8ull << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t parts = std::min<uint64_t>(std::min<uint64_t>(8, hw), n / PIECE);
+    if (parts <= 1) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const uint64_t step = ((n + parts - 1) / parts + 4095) & ~4095ull;
+    std::vector<std::thread> th;
+    for (uint64_t b = step; b < n; b += step)
+        th.emplace_back([=] { memcpy(dst + b, src + b, std::min(step, n - b)); });
+    memcpy(dst, src, std::min(step, n));
+    for (auto& t : th) t.join();
+}
+
 // A batch's result buffer, shared by its requests; freed with the last of them.
 struct ServeResult {
     void* p = nullptr;
@@ -54,7 +132,8 @@ struct ServeResult {
 
 struct ServeReq {
     uint64_t id = 0;
-    std::vector<uint8_t> text;  // host copy until the batch has uploaded it
+    std::vector<uint8_t> text;      // pageable host copy (when the pinned arena is full)
+    const uint8_t* pinned = nullptr;  // pinned host copy in the server's arena
     uint64_t n = 0;
     int dc = 0, width = 32;
     uint64_t footprint = 0;
@@ -67,8 +146,10 @@ struct ServeReq {
 
 class Server {
 public:
-    Server(const Ctx& parent, int lanes, uint64_t budget, uint64_t batch_bytes, uint32_t batch_texts)
-        : device_(parent.device), budget_(budget), batch_bytes_(batch_bytes), batch_texts_(batch_texts) {
+    Server(const Ctx& parent, int lanes, uint64_t budget, uint64_t batch_bytes, uint32_t batch_texts,
+           uint64_t host_bytes)
+        : device_(parent.device), budget_(budget), batch_bytes_(batch_bytes), batch_texts_(batch_texts),
+          arena_(host_bytes) {
         st_.lanes = (uint32_t)lanes;
         st_.budget_bytes = budget;
         for (int k = 0; k < lanes; k++) {
@@ -105,15 +186,22 @@ public:
             DcHost h;
             if (!make_dc((uint32_t)dc, h)) throw Error(DCX_ERR_ARG, "unsupported difference cover");
         }
+        const auto t_submit = std::chrono::steady_clock::now();
         const uint64_t fp = serve_footprint(n, width);
         if (fp > budget_) throw Error(DCX_ERR_BUDGET, "request footprint above the serving budget");
         auto r = std::make_unique<ServeReq>();
-        r->text.assign(text, text + n);
+        if (uint8_t* h = n ? arena_.alloc(n) : nullptr) {
+            parallel_copy(h, text, n);
+            r->pinned = h;
+        } else {
+            r->text.resize(n);
+            parallel_copy(r->text.data(), text, n);
+        }
         r->n = n;
         r->dc = dc;
         r->width = width;
         r->footprint = fp;
-        r->t_submit = std::chrono::steady_clock::now();
+        r->t_submit = t_submit;
         uint64_t id;
         {
             std::lock_guard<std::mutex> lk(mu_);
@@ -180,9 +268,14 @@ public:
         cv_work_.notify_all();
     }
 
+    // Waits until nothing is queued or running.  Throws DCX_ERR_BUDGET when the
+    // queue cannot move: nothing runs and the first request does not fit because
+    // unreleased results hold the budget.
     void drain() {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_done_.wait(lk, [&] { return queue_.empty() && running_ == 0; });
+        cv_done_.wait(lk, [&] { return (queue_.empty() && running_ == 0) || stalled(); });
+        if (!queue_.empty())
+            throw Error(DCX_ERR_BUDGET, "queued requests wait for results to be released");
     }
 
     dcx_serve_stats stats() {
@@ -195,6 +288,8 @@ public:
     }
 
 private:
+    bool stalled() const { return !queue_.empty() && running_ == 0 && !head_fits(); }
+
     bool head_fits() const {
         if (queue_.empty()) return false;
         const ServeReq& r = *reqs_.at(queue_.front());
@@ -256,6 +351,10 @@ private:
                     ServeReq* r = batch[i];
                     r->t_done = now;
                     std::vector<uint8_t>().swap(r->text);
+                    if (r->pinned) {
+                        arena_.free(r->pinned);
+                        r->pinned = nullptr;
+                    }
                     if (err == DCX_OK) {
                         r->status = 2;
                         r->res = res;
@@ -299,18 +398,34 @@ private:
             cudaFreeAsync(d_text, c.stream);
             throw Error(DCX_ERR_OOM, "result buffer");
         }
+        cudaEvent_t ev[3];
+        for (auto& e : ev) cudaEventCreate(&e);
+        cudaEventRecord(ev[0], c.stream);
         try {
             for (size_t i = 0; i < batch.size(); i++)
                 if (batch[i]->n)
-                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)d_text + offs[i], batch[i]->text.data(), batch[i]->n,
-                                             cudaMemcpyHostToDevice, c.stream));
+                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)d_text + offs[i],
+                                             batch[i]->pinned ? batch[i]->pinned : batch[i]->text.data(),
+                                             batch[i]->n, cudaMemcpyHostToDevice, c.stream));
+            cudaEventRecord(ev[1], c.stream);
             c.budget = c.in_use + scratch;  // build_batch sizes its rounds from this
             build_batch(c, (const uint8_t*)d_text, offs.data(), (uint32_t)batch.size(), dc, width, res->p,
                         DCX_DEVICE_PTRS);
+            cudaEventRecord(ev[2], c.stream);
             DCX_CUDA(cudaStreamSynchronize(c.stream));
         } catch (...) {
             cudaFreeAsync(d_text, c.stream);
+            for (auto& e : ev) cudaEventDestroy(e);
             throw;
+        }
+        float up = 0, bd = 0;
+        cudaEventElapsedTime(&up, ev[0], ev[1]);
+        cudaEventElapsedTime(&bd, ev[1], ev[2]);
+        for (auto& e : ev) cudaEventDestroy(e);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            st_.ms_upload += up;
+            st_.ms_build += bd;
         }
         DCX_CUDA(cudaFreeAsync(d_text, c.stream));
         return res;
@@ -319,6 +434,7 @@ private:
     int device_;
     uint64_t budget_, batch_bytes_;
     uint32_t batch_texts_;
+    PinnedArena arena_;
     std::mutex mu_, copy_mu_;
     std::condition_variable cv_work_, cv_done_;
     std::deque<uint64_t> queue_;

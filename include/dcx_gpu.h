@@ -158,6 +158,8 @@ typedef struct dcx_serve_stats {
     uint64_t max_batch_texts;     /* most requests in one batch */
     uint64_t queued;              /* requests waiting now */
     uint32_t running_batches;     /* batches on the GPU now */
+    double ms_upload;             /* summed over batches: host -> device copies of the texts */
+    double ms_build;              /* summed over batches: the builds */
 } dcx_serve_stats;
 
 /* Queues an SA request (dc = 0: DC39; sa_width 32, 40 or 64).  Returns
@@ -165,7 +167,9 @@ typedef struct dcx_serve_stats {
  * serving budget is the option "serve_budget" (bytes; 0 = the context budget),
  * read when the first request starts the server, as are "serve_lanes"
  * (default 3), "serve_batch_bytes" (text bytes per batch, default 1 GiB) and
- * "serve_batch_texts" (requests per batch, default 65536). */
+ * "serve_batch_texts" (requests per batch, default 65536) and
+ * "serve_host_bytes" (pinned host memory for request copies, default 8 GiB;
+ * requests that do not fit it are copied to pageable memory). */
 int dcx_serve_submit(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
                      uint64_t* req_id);
 /* Polls a request: *status = 0 queued, 1 running, 2 done, <0 failed (error code).
@@ -178,7 +182,9 @@ int dcx_serve_result_device(dcx_ctx* ctx, uint64_t req_id, const void** sa_dev);
 /* Frees a finished (or failed) request and its result; DCX_ERR_BUSY while it
  * is queued or running, DCX_ERR_NOTFOUND for unknown ids. */
 int dcx_serve_release(dcx_ctx* ctx, uint64_t req_id);
-/* Blocks until no request is queued or running. */
+/* Blocks until no request is queued or running.  Returns DCX_ERR_BUDGET instead
+ * of waiting forever when nothing runs and the first queued request cannot be
+ * admitted until results are released. */
 int dcx_serve_drain(dcx_ctx* ctx);
 int dcx_serve_get_stats(dcx_ctx* ctx, dcx_serve_stats* out);
 

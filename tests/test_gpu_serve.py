@@ -138,3 +138,25 @@ def test_serve_result_device(sctx):
     torch.cuda.synchronize()
     assert sctx.check_sa_device(d_text.data_ptr(), t.size, p, 32)
     sctx.serve_release(rid)
+
+
+def test_serve_drain_reports_stall(sctx, oracle):
+    """Unreleased results can hold the whole budget: drain then returns
+    DCX_ERR_BUDGET instead of waiting forever, and releases unblock the queue."""
+    from distributed_suffix_sorting_evaluation_b200 import DcxError
+    n = 100_000
+    fp = 48 * (n + 1) + (1 << 20) + ((n + 16 + 255) & ~255) + ((4 * n + 16 + 255) & ~255)
+    sctx.set_option("serve_budget", fp + (1 << 20))
+    sctx.set_option("serve_lanes", 1)
+    texts = [random_text(n, 4, seed=90 + i) for i in range(5)]
+    ids = [sctx.serve_submit(t, dc=0, sa_width=32) for t in texts]
+    with pytest.raises(DcxError) as e:
+        sctx.serve_drain()
+    assert e.value.code == -4
+    for rid, t in zip(ids[:3], texts[:3]):
+        assert np.array_equal(sctx.serve_result(rid, n, 32), oracle.libsais(t).astype(np.uint64))
+        sctx.serve_release(rid)
+    sctx.serve_drain()
+    for rid, t in zip(ids[3:], texts[3:]):
+        assert np.array_equal(sctx.serve_result(rid, n, 32), oracle.libsais(t).astype(np.uint64))
+        sctx.serve_release(rid)
