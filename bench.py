@@ -515,7 +515,9 @@ def run_serve(args, world, rank, local):
       plain     the per-request path on the capacity run's requests: one
                 dcx_build_sa per request on its slice already in HBM (no
                 upload), while --loop-budget-s lasts.
-    Texts are uploaded by the server (pageable host copies) inside the latency."""
+    Requests borrow slices of a pinned host copy of the text (zero-copy
+    submission; --serve-copy makes the server copy each text at submission);
+    the server's upload of each text is inside the latency."""
     import torch
     from distributed_suffix_sorting_evaluation_b200 import Context, SERVE_DONE, workloads as W
 
@@ -530,12 +532,17 @@ def run_serve(args, world, rank, local):
     lens = W.batch_lengths(count, 4 << 10, 256 << 20, seed=6).astype(np.int64)
     rng = np.random.default_rng(7 + rank)
     offs = (rng.random(count) * (base_n - lens)).astype(np.int64)
+    h_base = torch.from_numpy(base).pin_memory()
     ctx = Context(local)
     ctx.set_option("serve_budget", args.serve_budget_gb * 1e9)
     ctx.set_option("serve_lanes", args.serve_lanes)
+    borrow = not args.serve_copy
 
     def submit(i):
-        return ctx.serve_submit(None, dc=39, sa_width=32, text_ptr=base.ctypes.data + int(offs[i]), n=int(lens[i]))
+        # borrow: requests point into the pinned host text (zero-copy submission);
+        # copy: the server copies each text at submission (pinned arena)
+        return ctx.serve_submit(None, dc=39, sa_width=32, text_ptr=h_base.data_ptr() + int(offs[i]),
+                                n=int(lens[i]), borrow=borrow)
 
     # warm-up: a few requests of every size class through all lanes
     wids = [submit(i) for i in range(min(count, 3 * args.serve_lanes))]
@@ -551,6 +558,7 @@ def run_serve(args, world, rank, local):
         k += 1
     t0 = time.perf_counter()
     ids = [submit(i) for i in range(k)]
+    t_sub = time.perf_counter() - t0
     for r in ids:
         while True:
             st, _ = ctx.serve_poll(r)
@@ -624,7 +632,6 @@ def run_serve(args, world, rank, local):
     #        request uploaded from pinned host memory then built; latency =
     #        arrival -> SA complete in HBM, wall clock.
     d_base = torch.from_numpy(base).to(f"cuda:{local}")
-    h_base = torch.from_numpy(base).pin_memory()
     d_text = torch.empty(int(lens.max()) + 16, dtype=torch.uint8, device=f"cuda:{local}")
     d_sa = torch.empty(int(lens.max()) + 16, dtype=torch.int32, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
@@ -644,20 +651,23 @@ def run_serve(args, world, rank, local):
     plain = plain_bytes / GiB / (plain_ms / 1000.0)
     del d_base
     p_lat, p_bytes = [], 0
+    cur = torch.cuda.current_stream()
     start = time.perf_counter()
-    with torch.cuda.stream(stream):
-        for i in range(n_req):
-            t_arr = start + float(arr[i])
-            wait = t_arr - time.perf_counter()
-            if wait > 0:
-                time.sleep(wait)
-            n_i, o_i = int(lens[i % count]), int(offs[i % count])
-            d_text[:n_i].copy_(h_base[o_i:o_i + n_i], non_blocking=True)
-            ctx.build_sa_device(d_text.data_ptr(), n_i, d_sa.data_ptr(), dc=39, sa_width=32)
-            p_lat.append((time.perf_counter() - t_arr) * 1000.0)
-            p_bytes += n_i
+    for i in range(n_req):
+        t_arr = start + float(arr[i])
+        wait = t_arr - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        n_i, o_i = int(lens[i % count]), int(offs[i % count])
+        d_text[:n_i].copy_(h_base[o_i:o_i + n_i], non_blocking=True)
+        cur.synchronize()
+        ctx.build_sa_device(d_text.data_ptr(), n_i, d_sa.data_ptr(), dc=39, sa_width=32)
+        p_lat.append((time.perf_counter() - t_arr) * 1000.0)
+        p_bytes += n_i
     p_end = time.perf_counter()
     p_lat = np.array(p_lat)
+    torch.cuda.synchronize()
+    del d_text, d_sa, stream
 
     if rank == 0:
         line = {
@@ -667,6 +677,8 @@ def run_serve(args, world, rank, local):
             "data": "synthetic (slices of a seeded 1 GiB order-3 Markov DNA text, 5% repeats)",
             "config": {"workload": "cfg5_serve", "lengths": "log-uniform 4 KiB-256 MiB", "dc": 39, "sa_width": 32,
                        "budget_gb": args.serve_budget_gb, "lanes": args.serve_lanes,
+                       "submission": "borrow (zero-copy from pinned host text)" if borrow
+                       else "copy at submission (pinned arena)",
                        "arrivals": "Poisson at 80% of measured capacity",
                        "l2_flush": "batches up to 1 GiB of text, larger than L2",
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
@@ -677,7 +689,7 @@ def run_serve(args, world, rank, local):
             "offered": {"requests_per_s": round(rate, 2), "gib_per_s": round(0.8 * capacity, 4),
                         "seconds": round(served_s, 2), "bytes": int(done_bytes)},
             "capacity": {"value": round(capacity, 4), "unit": "GiB/s", "requests": k, "bytes": int(tot),
-                         "seconds": round(t_cap, 3)},
+                         "seconds": round(t_cap, 3), "submit_seconds": round(t_sub, 3)},
             "plain": {"value": round(plain, 4), "unit": "GiB/s", "requests": j, "bytes": plain_bytes,
                       "call": "dcx_build_sa per request on the capacity run's requests, device pointers, "
                               "text resident, device time",
@@ -720,6 +732,7 @@ def main():
     ap.add_argument("--serve-cap-gib", type=int, default=16, help="text of the closed-loop capacity run")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-lanes", type=int, default=3)
+    ap.add_argument("--serve-copy", action="store_true", help="copy texts at submission instead of borrowing")
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.workload == "cfg5_serve":

@@ -40,6 +40,7 @@ DCX_HOST_PTRS = 0
 DCX_DEVICE_PTRS = 1
 DCX_NO_PACKING = 2
 DCX_NO_REMAP = 4
+DCX_SERVE_BORROW = 8
 
 SUPPORTED_DC = (3, 7, 13, 21, 31, 39, 57, 73, 91, 95, 133)
 
@@ -49,6 +50,7 @@ EXPORTED = (
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
+    "dcx_serve_submit_ex",
 )
 
 # serving request states (dcx_serve_poll)
@@ -115,6 +117,7 @@ def load_library(path: str | None = None):
     lib.dcx_get_trace.argtypes = [vp, ctypes.POINTER(u64), vp, vp, u64]
     lib.dcx_build_sa_batch.argtypes = [vp, vp, vp, u32, i32, i32, vp, u32]
     lib.dcx_serve_submit.argtypes = [vp, vp, u64, i32, i32, ctypes.POINTER(u64)]
+    lib.dcx_serve_submit_ex.argtypes = [vp, vp, u64, i32, i32, u32, ctypes.POINTER(u64)]
     lib.dcx_serve_poll.argtypes = [vp, u64, vp, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]
     lib.dcx_serve_release.argtypes = [vp, u64]
     lib.dcx_serve_drain.argtypes = [vp]
@@ -277,16 +280,21 @@ class Context:
 
     # ---- serving -------------------------------------------------------------
     def serve_submit(self, text, dc: int = 0, sa_width: int = 32, text_ptr: int | None = None,
-                     n: int | None = None) -> int:
-        """Queues an SA request (the text is copied); returns its id.  Pass either
-        `text` (bytes / uint8 array) or a raw host pointer and length."""
+                     n: int | None = None, borrow: bool = False, device: bool = False) -> int:
+        """Queues an SA request; returns its id.  Pass either `text` (bytes /
+        uint8 array; copied) or a raw pointer and length.  borrow=True skips the
+        copy: the buffer must stay valid until the request is done; device=True
+        (with borrow) means a device pointer."""
         if text_ptr is None:
+            if borrow:
+                raise ValueError("borrow needs a raw pointer whose lifetime the caller controls")
             t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
                                      else np.asarray(text, dtype=np.uint8))
             text_ptr, n = (t.ctypes.data if t.size else None), t.size
+        flags = (DCX_SERVE_BORROW if borrow else 0) | (DCX_DEVICE_PTRS if device else 0)
         rid = ctypes.c_uint64()
-        _check(self.lib.dcx_serve_submit(self.h, ctypes.c_void_p(text_ptr) if text_ptr else None, n, dc, sa_width,
-                                         ctypes.byref(rid)))
+        _check(self.lib.dcx_serve_submit_ex(self.h, ctypes.c_void_p(text_ptr) if text_ptr else None, n, dc,
+                                            sa_width, flags, ctypes.byref(rid)))
         return rid.value
 
     def serve_poll(self, rid: int, out: np.ndarray | None = None):

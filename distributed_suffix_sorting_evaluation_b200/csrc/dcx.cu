@@ -1638,7 +1638,13 @@ static dcx::Server& server_of(dcx_ctx* x) {
 
 int dcx_serve_submit(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int sa_width, uint64_t* req_id) {
     if (!x || !req_id) return DCX_ERR_ARG;
-    return guarded([&] { *req_id = server_of(x).submit(text, n, dc, sa_width); });
+    return guarded([&] { *req_id = server_of(x).submit(text, n, dc, sa_width, 0); });
+}
+
+int dcx_serve_submit_ex(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int sa_width, uint32_t flags,
+                        uint64_t* req_id) {
+    if (!x || !req_id) return DCX_ERR_ARG;
+    return guarded([&] { *req_id = server_of(x).submit(text, n, dc, sa_width, flags); });
 }
 
 int dcx_serve_poll(dcx_ctx* x, uint64_t req_id, void* sa_host, int* status, double* latency_ms) {

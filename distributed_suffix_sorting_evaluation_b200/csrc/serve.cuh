@@ -132,8 +132,10 @@ struct ServeResult {
 
 struct ServeReq {
     uint64_t id = 0;
-    std::vector<uint8_t> text;      // pageable host copy (when the pinned arena is full)
+    std::unique_ptr<uint8_t[]> text;  // pageable host copy (when the pinned arena is full)
     const uint8_t* pinned = nullptr;  // pinned host copy in the server's arena
+    const uint8_t* borrowed = nullptr;  // caller's buffer (DCX_SERVE_BORROW), host or device
+    bool borrowed_dev = false;
     uint64_t n = 0;
     int dc = 0, width = 32;
     uint64_t footprint = 0;
@@ -178,7 +180,7 @@ public:
         cudaStreamDestroy(copy_stream_);
     }
 
-    uint64_t submit(const uint8_t* text, uint64_t n, int dc, int width) {
+    uint64_t submit(const uint8_t* text, uint64_t n, int dc, int width, uint32_t flags) {
         if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
         if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
         if (n && !text) throw Error(DCX_ERR_ARG, "null pointer");
@@ -190,12 +192,17 @@ public:
         const uint64_t fp = serve_footprint(n, width);
         if (fp > budget_) throw Error(DCX_ERR_BUDGET, "request footprint above the serving budget");
         auto r = std::make_unique<ServeReq>();
-        if (uint8_t* h = n ? arena_.alloc(n) : nullptr) {
+        if (flags & DCX_SERVE_BORROW) {
+            r->borrowed = text;
+            r->borrowed_dev = (flags & DCX_DEVICE_PTRS) != 0;
+        } else if (flags & DCX_DEVICE_PTRS) {
+            throw Error(DCX_ERR_ARG, "device texts are served only with DCX_SERVE_BORROW");
+        } else if (uint8_t* h = n ? arena_.alloc(n) : nullptr) {
             parallel_copy(h, text, n);
             r->pinned = h;
-        } else {
-            r->text.resize(n);
-            parallel_copy(r->text.data(), text, n);
+        } else if (n) {
+            r->text.reset(new uint8_t[n]);
+            parallel_copy(r->text.get(), text, n);
         }
         r->n = n;
         r->dc = dc;
@@ -350,7 +357,8 @@ private:
                 for (size_t i = 0; i < batch.size(); i++) {
                     ServeReq* r = batch[i];
                     r->t_done = now;
-                    std::vector<uint8_t>().swap(r->text);
+                    r->text.reset();
+                    r->borrowed = nullptr;
                     if (r->pinned) {
                         arena_.free(r->pinned);
                         r->pinned = nullptr;
@@ -382,6 +390,12 @@ private:
         }
     }
 
+    static const uint8_t* text_of(const ServeReq& r) {
+        if (r.borrowed) return r.borrowed;
+        if (r.pinned) return r.pinned;
+        return r.text.get();
+    }
+
     // Uploads the batch's texts, builds their SAs into one device buffer.
     std::shared_ptr<ServeResult> run(Ctx& c, const std::vector<ServeReq*>& batch, uint64_t scratch,
                                      std::vector<uint64_t>& offs) {
@@ -404,9 +418,10 @@ private:
         try {
             for (size_t i = 0; i < batch.size(); i++)
                 if (batch[i]->n)
-                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)d_text + offs[i],
-                                             batch[i]->pinned ? batch[i]->pinned : batch[i]->text.data(),
-                                             batch[i]->n, cudaMemcpyHostToDevice, c.stream));
+                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)d_text + offs[i], text_of(*batch[i]), batch[i]->n,
+                                             batch[i]->borrowed_dev ? cudaMemcpyDeviceToDevice
+                                                                    : cudaMemcpyHostToDevice,
+                                             c.stream));
             cudaEventRecord(ev[1], c.stream);
             c.budget = c.in_use + scratch;  // build_batch sizes its rounds from this
             build_batch(c, (const uint8_t*)d_text, offs.data(), (uint32_t)batch.size(), dc, width, res->p,

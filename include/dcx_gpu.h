@@ -172,6 +172,12 @@ typedef struct dcx_serve_stats {
  * requests that do not fit it are copied to pageable memory). */
 int dcx_serve_submit(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
                      uint64_t* req_id);
+/* dcx_serve_submit with flags: DCX_SERVE_BORROW skips the copy at submission --
+ * the caller keeps `text` valid and unchanged until the request is done (or
+ * failed); with DCX_SERVE_BORROW | DCX_DEVICE_PTRS the text is a device buffer. */
+#define DCX_SERVE_BORROW 8
+int dcx_serve_submit_ex(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
+                        uint32_t flags, uint64_t* req_id);
 /* Polls a request: *status = 0 queued, 1 running, 2 done, <0 failed (error code).
  * When done and sa_host is non-null, copies the SA (n entries of sa_width bits)
  * into sa_host.  latency_ms (optional) receives the submit -> done time (done =

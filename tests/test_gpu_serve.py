@@ -160,3 +160,17 @@ def test_serve_drain_reports_stall(sctx, oracle):
     for rid, t in zip(ids[3:], texts[3:]):
         assert np.array_equal(sctx.serve_result(rid, n, 32), oracle.libsais(t).astype(np.uint64))
         sctx.serve_release(rid)
+
+
+def test_serve_borrowed_host_and_device(sctx, oracle):
+    """Zero-copy submissions: borrowed host and device buffers give the same SAs."""
+    import torch
+    texts = [random_text(n, 4, seed=300 + n) for n in (5, 4_000, 120_000)]
+    hbufs = [torch.from_numpy(t.copy()).pin_memory() for t in texts]
+    dbufs = [torch.from_numpy(t.copy()).cuda() for t in texts]
+    torch.cuda.synchronize()
+    ids = [sctx.serve_submit(None, text_ptr=h.data_ptr(), n=h.numel(), borrow=True) for h in hbufs]
+    ids += [sctx.serve_submit(None, text_ptr=d.data_ptr(), n=d.numel(), borrow=True, device=True) for d in dbufs]
+    for rid, t in zip(ids, texts + texts):
+        assert np.array_equal(sctx.serve_result(rid, t.size, 32), oracle.libsais(t).astype(np.uint64))
+        sctx.serve_release(rid)
