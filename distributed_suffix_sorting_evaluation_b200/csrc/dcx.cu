@@ -202,11 +202,12 @@ struct Options {
     uint32_t spin_limit = 1u << 24;
     uint64_t batch_round_cap = 0;  // max elements per batch round (0 = from the budget)
     // serving
-    uint32_t serve_lanes = 3;
+    uint32_t serve_lanes = 2;
     uint64_t serve_budget = 0;  // 0 = the context budget
     uint64_t serve_batch_bytes = 1ull << 30;
     uint32_t serve_batch_texts = 65536;
     uint64_t serve_host_bytes = 8ull << 30;  // pinned host arena for request copies
+    uint64_t serve_express_bytes = 4ull << 20;  // longest request the express lanes take
 };
 
 struct Ctx;
@@ -244,6 +245,7 @@ struct Ctx {
     size_t lookback_tiles = 0;
     uint32_t epoch = 0;
     uint32_t* h_pinned = nullptr;   // pinned staging for small transfers (PINNED_WORDS words)
+    cudaMemPool_t pool = nullptr;   // own memory pool (serving lanes); null = the device's default pool
     std::map<uint32_t, DcHost> dc_host;
     std::map<uint32_t, DcFlags*> dc_flags_dev;  // per X (samples_before filled per level on a copy)
     std::map<uint32_t, DcDev*> dc_dev;
@@ -259,7 +261,7 @@ struct Ctx {
         if (budget && in_use + bytes > budget)
             throw Error(DCX_ERR_BUDGET, "device footprint above the context budget");
         void* p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, stream) : cudaMallocAsync(&p, bytes, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw Error(DCX_ERR_OOM, "cudaMallocAsync failed for " + std::to_string(bytes) + " bytes");
@@ -372,6 +374,7 @@ struct SortSpace {
 };
 
 static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
+    if (kw > 3) throw Error(DCX_ERR_INTERNAL, "radix keys wider than 3 words");
     const uint32_t passes = 4 * kw;
     // histograms in and digit bases out through pinned staging (PINNED_WORDS words each)
     uint32_t* h = reinterpret_cast<uint32_t*>(c.h_pinned);
@@ -392,8 +395,8 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         }
     }
     if (run.empty()) return 0;
-    constexpr int ITEMS = 12;  // 64 registers: 4 CTAs per SM (measured best on B200)
-    constexpr int TILE = SORT_THREADS * ITEMS;
+    constexpr int ITEMS = ONESWEEP_ITEMS;
+    constexpr int TILE = ONESWEEP_TILE;
     const uint64_t tiles = div_up(count, TILE);
     if (tiles > c.lookback_tiles) {
         if (c.d_lookback) DCX_CUDA(cudaFree(c.d_lookback));
@@ -412,6 +415,14 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
     cudaEventCreate(&e1);
     cudaEventRecord(e0, c.stream);
     int cur = 0;
+    const size_t smem = onesweep_st_smem(kw);
+    DCX_CUDA(cudaFuncSetAttribute(k_onesweep_st<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)onesweep_st_smem(3)));
+    bool aligned16 = true;
+    for (int b = 0; b < 2; b++) {
+        for (uint32_t w = 0; w < kw; w++) aligned16 &= ((uintptr_t)s.k[b][w] & 15) == 0;
+        aligned16 &= ((uintptr_t)s.v[b] & 15) == 0;
+    }
     for (size_t i = 0; i < run.size(); i++) {
         if (++c.epoch >= (1u << 30)) {
             DCX_CUDA(cudaMemsetAsync(c.d_lookback, 0, c.lookback_tiles * RADIX * sizeof(uint64_t), c.stream));
@@ -433,7 +444,7 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         a.epoch = c.epoch;
         a.err = c.d_err;
         a.spin_limit = c.opt.spin_limit;
-        k_onesweep_ec<ITEMS, true><<<(unsigned)tiles, SORT_THREADS, 0, c.stream>>>(a);
+        k_onesweep_st<ITEMS><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a, aligned16);
         DCX_CHECK_LAUNCH();
         cur ^= 1;
     }
@@ -1554,6 +1565,7 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
         o.serve_lanes = (uint32_t)value;
     } else if (s == "serve_budget") o.serve_budget = (uint64_t)value;
     else if (s == "serve_host_bytes") o.serve_host_bytes = (uint64_t)value;
+    else if (s == "serve_express_bytes") o.serve_express_bytes = (uint64_t)value;
     else if (s == "serve_batch_bytes") {
         if (value < 1) return DCX_ERR_ARG;
         o.serve_batch_bytes = (uint64_t)value;
@@ -1631,7 +1643,7 @@ static dcx::Server& server_of(dcx_ctx* x) {
         const dcx::Options& o = x->c.opt;
         const uint64_t budget = o.serve_budget ? o.serve_budget : x->c.budget;
         x->server = std::make_unique<dcx::Server>(x->c, (int)o.serve_lanes, budget, o.serve_batch_bytes,
-                                                  o.serve_batch_texts, o.serve_host_bytes);
+                                                  o.serve_batch_texts, o.serve_host_bytes, o.serve_express_bytes);
     }
     return *x->server;
 }

@@ -149,6 +149,13 @@ constexpr int SLIDE_R = 16;
 constexpr int SLIDE_TILE = SLIDE_THREADS * SLIDE_R;
 constexpr int SLIDE_MAX_CHARS = 64;
 
+// Padded shared-memory indices: thread t works on positions [16t, 16t+16), so
+// unpadded rows of 16 keys (128 B) or 16 chars (16 B) would put a warp's lanes
+// on the same banks.  One spare key per 16 keys and 4 spare bytes per 16 chars
+// spread the lanes over the banks.
+__device__ __forceinline__ uint32_t slide_kidx(uint32_t i) { return i + (i >> 4); }
+__device__ __forceinline__ uint32_t slide_cidx(uint32_t i) { return i + ((i >> 4) << 2); }
+
 template <bool SEG, typename CharT>
 __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __restrict__ text, uint64_t N, SegView sv,
                                                               KeyPlan plan, uint64_t pow_top, uint64_t seg_mul,
@@ -156,8 +163,8 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
                                                               uint32_t* hist) {
     extern __shared__ uint32_t sh[];  // HIST_COPIES * 8 * RADIX histogram words, then the staging area
     uint32_t* hst = sh;
-    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 8 * RADIX);  // SLIDE_TILE keys
-    CharT* s_chars = reinterpret_cast<CharT*>(s_keys + SLIDE_TILE);                // SLIDE_TILE + P chars
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 8 * RADIX);  // SLIDE_TILE keys, padded
+    CharT* s_chars = reinterpret_cast<CharT*>(s_keys + SLIDE_TILE + SLIDE_TILE / 16);  // SLIDE_TILE + P, padded
     const uint32_t W = plan.kw;
     hist_zero(hst, 4 * W * RADIX);
     const uint32_t P = plan.chars;
@@ -165,7 +172,7 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
     for (uint64_t base = (uint64_t)blockIdx.x * SLIDE_TILE; base < N; base += (uint64_t)gridDim.x * SLIDE_TILE) {
         for (uint32_t i = threadIdx.x; i < SLIDE_TILE + P; i += SLIDE_THREADS) {
             const uint64_t p = base + i;
-            s_chars[i] = p < N ? text[p] : CharT(0);
+            s_chars[slide_cidx(i)] = p < N ? text[p] : CharT(0);
         }
         __syncthreads();
         const uint32_t r0 = threadIdx.x * SLIDE_R;
@@ -173,14 +180,15 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
         uint64_t end = seg_end(sv, sg);  // position of the text's 0
         auto full = [&](uint32_t r) {     // window of tile position r, cut at `end`
             uint64_t k = 0;
-            for (uint32_t j = 0; j < P; j++) k = k * B + ((base + r + j < end) ? (uint32_t)s_chars[r + j] : 0u);
+            for (uint32_t j = 0; j < P; j++)
+                k = k * B + ((base + r + j < end) ? (uint32_t)s_chars[slide_cidx(r + j)] : 0u);
             return k;
         };
         uint64_t key = full(r0);
 #pragma unroll
         for (int r = 0; r < SLIDE_R; r++) {
             const uint64_t i = base + r0 + r;
-            s_keys[r0 + r] = SEG ? key + (uint64_t)sg * seg_mul : key;  // text * B^P + window
+            s_keys[slide_kidx(r0 + r)] = SEG ? key + (uint64_t)sg * seg_mul : key;  // text * B^P + window
             if (i == end) {  // next position starts the next text
                 if (SEG && sg + 1 < sv.K) {
                     sg++;
@@ -188,15 +196,15 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
                 }
                 key = full(r0 + r + 1);
             } else {
-                const uint32_t out = (uint32_t)s_chars[r0 + r];
-                const uint32_t in = (i + P < end) ? (uint32_t)s_chars[r0 + r + P] : 0u;
+                const uint32_t out = (uint32_t)s_chars[slide_cidx(r0 + r)];
+                const uint32_t in = (i + P < end) ? (uint32_t)s_chars[slide_cidx(r0 + r + P)] : 0u;
                 key = (key - (uint64_t)out * pow_top) * B + in;
             }
         }
         __syncthreads();
         const uint32_t tile_n = (uint32_t)((N - base) < SLIDE_TILE ? (N - base) : SLIDE_TILE);
         for (uint32_t i = threadIdx.x; i < tile_n; i += SLIDE_THREADS) {
-            const uint64_t k = s_keys[i];
+            const uint64_t k = s_keys[slide_kidx(i)];
             uint32_t kk[2] = {(uint32_t)k, (uint32_t)(k >> 32)};
             ko.w[0][base + i] = kk[0];
             if (W > 1) ko.w[1][base + i] = kk[1];
@@ -211,8 +219,8 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
 
 template <typename CharT>
 constexpr size_t keys_slide_smem() {
-    return sizeof(uint32_t) * HIST_COPIES * 8 * RADIX + sizeof(uint64_t) * SLIDE_TILE +
-           sizeof(CharT) * (SLIDE_TILE + SLIDE_MAX_CHARS);
+    return sizeof(uint32_t) * HIST_COPIES * 8 * RADIX + sizeof(uint64_t) * (SLIDE_TILE + SLIDE_TILE / 16) +
+           sizeof(CharT) * (SLIDE_TILE + SLIDE_MAX_CHARS) * 5 / 4 + 64;
 }
 
 // Text id of every sorted element: the key is text-major and text s has

@@ -7,6 +7,9 @@
 //   * L lanes (threads, each with its own stream and scratch context) take
 //     work whenever they are free, so requests arriving while other batches
 //     run start at once on a free lane and overlap with them on the device;
+//     lane 0 takes any request, the others only short ones (size classes), so
+//     long builds never contend with each other and short ones never queue
+//     behind them;
 //   * a lane admits the queued requests of one (dc, sa_width) class, first come
 //     first served, while their projected footprint fits the HBM budget and the
 //     batch stays under a text-byte cap; a request that does not fit waits for
@@ -149,8 +152,9 @@ struct ServeReq {
 class Server {
 public:
     Server(const Ctx& parent, int lanes, uint64_t budget, uint64_t batch_bytes, uint32_t batch_texts,
-           uint64_t host_bytes)
+           uint64_t host_bytes, uint64_t express_bytes)
         : device_(parent.device), budget_(budget), batch_bytes_(batch_bytes), batch_texts_(batch_texts),
+          express_bytes_(express_bytes), express_batch_bytes_(std::max<uint64_t>(4 * express_bytes, 1 << 20)),
           arena_(host_bytes) {
         st_.lanes = (uint32_t)lanes;
         st_.budget_bytes = budget;
@@ -159,6 +163,22 @@ public:
             ctx_init(*c, device_, 0);
             c->opt = parent.opt;
             c->opt.trace = 0;
+            // Each lane allocates from its own pool: a shared pool would hand one
+            // lane's freed block to another and make its stream wait for the
+            // first lane's work, serialising the lanes.
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = device_;
+            DCX_CUDA(cudaMemPoolCreate(&c->pool, &props));
+            uint64_t thr = UINT64_MAX;
+            DCX_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr));
+            if (k > 0) {  // express lanes: short builds get the SMs first when both lanes have work ready
+                int least = 0, greatest = 0;
+                DCX_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+                DCX_CUDA(cudaStreamDestroy(c->stream));
+                DCX_CUDA(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, greatest));
+            }
             lanes_.push_back(std::move(c));
         }
         DCX_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
@@ -175,7 +195,9 @@ public:
         reqs_.clear();  // frees the results on their lanes' streams
         for (auto& c : lanes_) {
             cudaStreamSynchronize(c->stream);
+            cudaMemPool_t pool = c->pool;
             ctx_free(*c);
+            if (pool) cudaMemPoolDestroy(pool);
         }
         cudaStreamDestroy(copy_stream_);
     }
@@ -295,12 +317,28 @@ public:
     }
 
 private:
-    bool stalled() const { return !queue_.empty() && running_ == 0 && !head_fits(); }
+    // Lane 0 is the bulk lane: it serves the queue in arrival order, any size.
+    // Lanes 1.. are express lanes: they serve only requests of at most
+    // express_bytes (in arrival order among those), so short requests do not
+    // wait behind long batches, while long requests never run two at a time
+    // and contend for the GPU.
+    bool admissible(int lane, const ServeReq& r) const { return lane == 0 || r.n <= express_bytes_; }
 
-    bool head_fits() const {
-        if (queue_.empty()) return false;
-        const ServeReq& r = *reqs_.at(queue_.front());
-        return reserved_ + r.footprint <= budget_;
+    // First queued request lane `lane` may start now (it fits the budget), or null.
+    const ServeReq* first_for(int lane) const {
+        for (uint64_t id : queue_) {
+            const ServeReq& r = *reqs_.at(id);
+            if (!admissible(lane, r)) continue;
+            return reserved_ + r.footprint <= budget_ ? &r : nullptr;  // first come, first served
+        }
+        return nullptr;
+    }
+
+    bool stalled() const {
+        if (queue_.empty() || running_ != 0) return false;
+        for (int k = 0; k < (int)lanes_.size(); k++)
+            if (first_for(k)) return false;
+        return true;
     }
 
     void lane_main(int k) {
@@ -311,18 +349,18 @@ private:
             uint64_t scratch = 0, text_bytes = 0;
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_work_.wait(lk, [&] { return stop_ || head_fits(); });
+                cv_work_.wait(lk, [&] { return stop_ || first_for(k) != nullptr; });
                 if (stop_) return;
-                const ServeReq& head = *reqs_.at(queue_.front());
+                const ServeReq& head = *first_for(k);
                 const int dc = head.dc, width = head.width;
+                const uint64_t cap = k == 0 ? batch_bytes_ : std::min(batch_bytes_, express_batch_bytes_);
                 for (auto it = queue_.begin(); it != queue_.end();) {
                     ServeReq* r = reqs_.at(*it).get();
-                    if (r->dc != dc || r->width != width) {  // another class: left for the next lane
+                    if (r->dc != dc || r->width != width || !admissible(k, *r)) {  // left for another lane
                         ++it;
                         continue;
                     }
-                    if (!batch.empty() &&
-                        (text_bytes + r->n > batch_bytes_ || batch.size() >= batch_texts_))
+                    if (!batch.empty() && (text_bytes + r->n > cap || batch.size() >= batch_texts_))
                         break;
                     if (reserved_ + r->footprint > budget_) break;  // first come, first served
                     reserved_ += r->footprint;
@@ -406,8 +444,8 @@ private:
         res->stream = c.stream;
         res->bytes = serve_result_bytes(total, width);
         void* d_text = nullptr;
-        DCX_CUDA(cudaMallocAsync(&d_text, total + 16, c.stream));
-        if (cudaMallocAsync(&res->p, res->bytes, c.stream) != cudaSuccess) {
+        DCX_CUDA(cudaMallocFromPoolAsync(&d_text, total + 16, c.pool, c.stream));
+        if (cudaMallocFromPoolAsync(&res->p, res->bytes, c.pool, c.stream) != cudaSuccess) {
             cudaGetLastError();
             cudaFreeAsync(d_text, c.stream);
             throw Error(DCX_ERR_OOM, "result buffer");
@@ -449,6 +487,7 @@ private:
     int device_;
     uint64_t budget_, batch_bytes_;
     uint32_t batch_texts_;
+    uint64_t express_bytes_, express_batch_bytes_;
     PinnedArena arena_;
     std::mutex mu_, copy_mu_;
     std::condition_variable cv_work_, cv_done_;
