@@ -536,6 +536,7 @@ def run_serve(args, world, rank, local):
     ctx = Context(local)
     ctx.set_option("serve_budget", args.serve_budget_gb * 1e9)
     ctx.set_option("serve_lanes", args.serve_lanes)
+    ctx.set_option("serve_express_priority", args.serve_express_priority)
     borrow = not args.serve_copy
 
     def submit(i):
@@ -698,6 +699,7 @@ def run_serve(args, world, rank, local):
             "data": "synthetic (slices of a seeded 1 GiB order-3 Markov DNA text, 5% repeats)",
             "config": {"workload": "cfg5_serve", "lengths": "log-uniform 4 KiB-256 MiB", "dc": 39, "sa_width": 32,
                        "budget_gb": args.serve_budget_gb, "lanes": args.serve_lanes,
+                       "express_priority": args.serve_express_priority,
                        "submission": "borrow (zero-copy from pinned host text)" if borrow
                        else "copy at submission (pinned arena)",
                        "arrivals": "Poisson at 80% of measured capacity",
@@ -757,8 +759,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="open-loop arrival window")
     ap.add_argument("--serve-cap-gib", type=int, default=16, help="text of the closed-loop capacity run")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
-    ap.add_argument("--serve-lanes", type=int, default=2)
+    ap.add_argument("--serve-lanes", type=int, default=1)
     ap.add_argument("--serve-copy", action="store_true", help="copy texts at submission instead of borrowing")
+    ap.add_argument("--serve-express-priority", type=int, default=1)
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.workload == "cfg5_serve":

@@ -202,12 +202,13 @@ struct Options {
     uint32_t spin_limit = 1u << 24;
     uint64_t batch_round_cap = 0;  // max elements per batch round (0 = from the budget)
     // serving
-    uint32_t serve_lanes = 2;
+    uint32_t serve_lanes = 1;
     uint64_t serve_budget = 0;  // 0 = the context budget
     uint64_t serve_batch_bytes = 1ull << 30;
     uint32_t serve_batch_texts = 65536;
     uint64_t serve_host_bytes = 8ull << 30;  // pinned host arena for request copies
     uint64_t serve_express_bytes = 4ull << 20;  // longest request the express lanes take
+    int serve_express_priority = 1;               // express lanes on high-priority streams
 };
 
 struct Ctx;
@@ -1566,6 +1567,7 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
     } else if (s == "serve_budget") o.serve_budget = (uint64_t)value;
     else if (s == "serve_host_bytes") o.serve_host_bytes = (uint64_t)value;
     else if (s == "serve_express_bytes") o.serve_express_bytes = (uint64_t)value;
+    else if (s == "serve_express_priority") o.serve_express_priority = value != 0;
     else if (s == "serve_batch_bytes") {
         if (value < 1) return DCX_ERR_ARG;
         o.serve_batch_bytes = (uint64_t)value;
@@ -1643,7 +1645,8 @@ static dcx::Server& server_of(dcx_ctx* x) {
         const dcx::Options& o = x->c.opt;
         const uint64_t budget = o.serve_budget ? o.serve_budget : x->c.budget;
         x->server = std::make_unique<dcx::Server>(x->c, (int)o.serve_lanes, budget, o.serve_batch_bytes,
-                                                  o.serve_batch_texts, o.serve_host_bytes, o.serve_express_bytes);
+                                                  o.serve_batch_texts, o.serve_host_bytes, o.serve_express_bytes,
+                                                  o.serve_express_priority != 0);
     }
     return *x->server;
 }

@@ -7,9 +7,10 @@
 //   * L lanes (threads, each with its own stream and scratch context) take
 //     work whenever they are free, so requests arriving while other batches
 //     run start at once on a free lane and overlap with them on the device;
-//     lane 0 takes any request, the others only short ones (size classes), so
-//     long builds never contend with each other and short ones never queue
-//     behind them;
+//     lane 0 (bulk) takes the long requests, the others (express, on
+//     high-priority streams) the short ones, so long builds never contend with
+//     each other and short ones never queue behind them; the bulk lane uploads
+//     its next batch while it builds the current one;
 //   * a lane admits the queued requests of one (dc, sa_width) class, first come
 //     first served, while their projected footprint fits the HBM budget and the
 //     batch stays under a text-byte cap; a request that does not fit waits for
@@ -152,7 +153,7 @@ struct ServeReq {
 class Server {
 public:
     Server(const Ctx& parent, int lanes, uint64_t budget, uint64_t batch_bytes, uint32_t batch_texts,
-           uint64_t host_bytes, uint64_t express_bytes)
+           uint64_t host_bytes, uint64_t express_bytes, bool express_priority)
         : device_(parent.device), budget_(budget), batch_bytes_(batch_bytes), batch_texts_(batch_texts),
           express_bytes_(express_bytes), express_batch_bytes_(std::max<uint64_t>(4 * express_bytes, 1 << 20)),
           arena_(host_bytes) {
@@ -173,12 +174,15 @@ public:
             DCX_CUDA(cudaMemPoolCreate(&c->pool, &props));
             uint64_t thr = UINT64_MAX;
             DCX_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr));
-            if (k > 0) {  // express lanes: short builds get the SMs first when both lanes have work ready
+            if (k > 0 && express_priority) {  // express lanes: short builds get the SMs first
                 int least = 0, greatest = 0;
                 DCX_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
                 DCX_CUDA(cudaStreamDestroy(c->stream));
                 DCX_CUDA(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, greatest));
             }
+            cudaStream_t cs;
+            DCX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            copy_streams_.push_back(cs);
             lanes_.push_back(std::move(c));
         }
         DCX_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
@@ -193,10 +197,13 @@ public:
         cv_work_.notify_all();
         for (auto& t : threads_) t.join();
         reqs_.clear();  // frees the results on their lanes' streams
-        for (auto& c : lanes_) {
-            cudaStreamSynchronize(c->stream);
-            cudaMemPool_t pool = c->pool;
-            ctx_free(*c);
+        for (size_t k = 0; k < lanes_.size(); k++) {
+            Ctx& c = *lanes_[k];
+            cudaStreamSynchronize(copy_streams_[k]);
+            cudaStreamSynchronize(c.stream);
+            cudaStreamDestroy(copy_streams_[k]);
+            cudaMemPool_t pool = c.pool;
+            ctx_free(c);
             if (pool) cudaMemPoolDestroy(pool);
         }
         cudaStreamDestroy(copy_stream_);
@@ -317,12 +324,15 @@ public:
     }
 
 private:
-    // Lane 0 is the bulk lane: it serves the queue in arrival order, any size.
-    // Lanes 1.. are express lanes: they serve only requests of at most
-    // express_bytes (in arrival order among those), so short requests do not
-    // wait behind long batches, while long requests never run two at a time
-    // and contend for the GPU.
-    bool admissible(int lane, const ServeReq& r) const { return lane == 0 || r.n <= express_bytes_; }
+    // Lane 0 is the bulk lane: it serves the requests longer than express_bytes
+    // (every request when it is the only lane).  Lanes 1.. are express lanes:
+    // they serve only requests of at most express_bytes.  Each class is served
+    // in arrival order; short requests never wait behind long batches, and long
+    // builds never run two at a time and contend for the GPU.
+    bool admissible(int lane, const ServeReq& r) const {
+        if (lanes_.size() == 1) return true;
+        return lane == 0 ? r.n > express_bytes_ : r.n <= express_bytes_;
+    }
 
     // First queued request lane `lane` may start now (it fits the budget), or null.
     const ServeReq* first_for(int lane) const {
@@ -341,147 +351,218 @@ private:
         return true;
     }
 
+    // A batch taken from the queue: its requests, reserved scratch and (once
+    // uploaded) the device copy of its texts.
+    struct Batch {
+        std::vector<ServeReq*> reqs;
+        uint64_t scratch = 0;
+        std::vector<uint64_t> offs;
+        void* d_text = nullptr;
+        cudaEvent_t ev_up0 = nullptr, ev_up1 = nullptr;  // around the upload (copy stream)
+        int err = DCX_OK;
+        bool empty() const { return reqs.empty(); }
+    };
+
+    // Takes the queued requests lane k may start now (one (dc, width) class,
+    // arrival order, within the budget and the lane's batch cap).  `block`:
+    // wait for work; otherwise return an empty batch when none is ready.
+    // Returns false only when the server stops.
+    bool admit(int k, bool block, Batch& b) {
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            if (block) cv_work_.wait(lk, [&] { return stop_ || first_for(k) != nullptr; });
+            if (stop_) return false;
+            const ServeReq* head = first_for(k);
+            if (!head) return true;
+            const int dc = head->dc, width = head->width;
+            const uint64_t cap = k == 0 ? batch_bytes_ : std::min(batch_bytes_, express_batch_bytes_);
+            uint64_t text_bytes = 0;
+            for (auto it = queue_.begin(); it != queue_.end();) {
+                ServeReq* r = reqs_.at(*it).get();
+                if (r->dc != dc || r->width != width || !admissible(k, *r)) {  // left for another lane
+                    ++it;
+                    continue;
+                }
+                if (!b.reqs.empty() && (text_bytes + r->n > cap || b.reqs.size() >= batch_texts_)) break;
+                if (reserved_ + r->footprint > budget_) break;  // first come, first served
+                reserved_ += r->footprint;
+                b.scratch += r->footprint - serve_result_bytes(r->n, width);
+                text_bytes += r->n;
+                r->status = 1;
+                r->lane = k;
+                r->t_start = std::chrono::steady_clock::now();
+                b.reqs.push_back(r);
+                it = queue_.erase(it);
+            }
+            running_++;
+            st_.batches++;
+            st_.peak_reserved_bytes = std::max<uint64_t>(st_.peak_reserved_bytes, reserved_);
+            st_.max_batch_texts = std::max<uint64_t>(st_.max_batch_texts, b.reqs.size());
+        }
+        cv_work_.notify_all();  // the rest of the queue may fit another lane
+        return true;
+    }
+
+    // Enqueues the copies of the batch's texts on the lane's copy stream.
+    void upload(int k, Batch& b) {
+        Ctx& c = *lanes_[k];
+        cudaStream_t cs = copy_streams_[k];
+        b.offs.assign(b.reqs.size() + 1, 0);
+        for (size_t i = 0; i < b.reqs.size(); i++) b.offs[i + 1] = b.offs[i] + b.reqs[i]->n;
+        try {
+            DCX_CUDA(cudaEventCreate(&b.ev_up0));
+            DCX_CUDA(cudaEventCreate(&b.ev_up1));
+            DCX_CUDA(cudaMallocFromPoolAsync(&b.d_text, b.offs.back() + 16, c.pool, cs));
+            DCX_CUDA(cudaEventRecord(b.ev_up0, cs));
+            for (size_t i = 0; i < b.reqs.size(); i++)
+                if (b.reqs[i]->n)
+                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)b.d_text + b.offs[i], text_of(*b.reqs[i]), b.reqs[i]->n,
+                                             b.reqs[i]->borrowed_dev ? cudaMemcpyDeviceToDevice
+                                                                     : cudaMemcpyHostToDevice,
+                                             cs));
+            DCX_CUDA(cudaEventRecord(b.ev_up1, cs));
+        } catch (const Error& e) {
+            b.err = e.code;
+        }
+    }
+
+    // Builds an uploaded batch on the lane's stream; returns the result buffer.
+    std::shared_ptr<ServeResult> build(int k, Batch& b) {
+        Ctx& c = *lanes_[k];
+        if (b.err != DCX_OK) throw Error(b.err, "upload failed");
+        const int width = b.reqs[0]->width, dc = b.reqs[0]->dc;
+        auto res = std::make_shared<ServeResult>();
+        res->stream = c.stream;
+        res->bytes = serve_result_bytes(b.offs.back(), width);
+        DCX_CUDA(cudaStreamWaitEvent(c.stream, b.ev_up1, 0));
+        if (cudaMallocFromPoolAsync(&res->p, res->bytes, c.pool, c.stream) != cudaSuccess) {
+            cudaGetLastError();
+            res->p = nullptr;
+            throw Error(DCX_ERR_OOM, "result buffer");
+        }
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, c.stream);
+        try {
+            c.budget = c.in_use + b.scratch;  // build_batch sizes its rounds from this
+            build_batch(c, (const uint8_t*)b.d_text, b.offs.data(), (uint32_t)b.reqs.size(), dc, width, res->p,
+                        DCX_DEVICE_PTRS);
+            cudaEventRecord(e1, c.stream);
+            DCX_CUDA(cudaStreamSynchronize(c.stream));
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        float up = 0, bd = 0;
+        cudaEventElapsedTime(&up, b.ev_up0, b.ev_up1);
+        cudaEventElapsedTime(&bd, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        std::lock_guard<std::mutex> lk(mu_);
+        st_.ms_upload += up;
+        st_.ms_build += bd;
+        return res;
+    }
+
+    // Frees the batch's upload state (ordered after the lane's work on it).
+    void drop_upload(int k, Batch& b) {
+        Ctx& c = *lanes_[k];
+        if (b.d_text) {
+            cudaStreamWaitEvent(c.stream, b.ev_up1, 0);
+            cudaFreeAsync(b.d_text, c.stream);
+        }
+        if (b.ev_up0) cudaEventDestroy(b.ev_up0);
+        if (b.ev_up1) cudaEventDestroy(b.ev_up1);
+        b.d_text = nullptr;
+        b.ev_up0 = b.ev_up1 = nullptr;
+    }
+
+    void complete(int k, Batch& b, const std::shared_ptr<ServeResult>& res, int err) {
+        Ctx& c = *lanes_[k];
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            const auto now = std::chrono::steady_clock::now();
+            uint64_t result_bytes = 0;
+            for (size_t i = 0; i < b.reqs.size(); i++) {
+                ServeReq* r = b.reqs[i];
+                r->t_done = now;
+                r->text.reset();
+                r->borrowed = nullptr;
+                if (r->pinned) {
+                    arena_.free(r->pinned);
+                    r->pinned = nullptr;
+                }
+                if (err == DCX_OK) {
+                    r->status = 2;
+                    r->res = res;
+                    r->res_off = b.offs[i] * (uint64_t)(r->width / 8);
+                    st_.done++;
+                    st_.done_bytes += r->n;
+                } else {
+                    r->status = err;
+                    st_.failed++;
+                }
+            }
+            if (err == DCX_OK && res) {
+                res->refs = (uint32_t)b.reqs.size();
+                result_bytes = res->bytes;
+            }
+            // the scratch and text parts end with the batch, the result stays until released
+            uint64_t fp = 0;
+            for (ServeReq* r : b.reqs) fp += r->footprint;
+            reserved_ -= fp - result_bytes;
+            st_.peak_lane_bytes = std::max<uint64_t>(st_.peak_lane_bytes, c.peak);
+            running_--;
+        }
+        cv_work_.notify_all();
+        cv_done_.notify_all();
+    }
+
+    // Lane loop.  The bulk lane prefetches: once a batch is uploaded it takes
+    // the next one from the queue and enqueues its upload on the copy stream
+    // before building the current one, so uploads overlap builds.
     void lane_main(int k) {
         cudaSetDevice(device_);
-        Ctx& c = *lanes_[k];
+        Batch cur, nxt;
         for (;;) {
-            std::vector<ServeReq*> batch;
-            uint64_t scratch = 0, text_bytes = 0;
-            {
-                std::unique_lock<std::mutex> lk(mu_);
-                cv_work_.wait(lk, [&] { return stop_ || first_for(k) != nullptr; });
-                if (stop_) return;
-                const ServeReq& head = *first_for(k);
-                const int dc = head.dc, width = head.width;
-                const uint64_t cap = k == 0 ? batch_bytes_ : std::min(batch_bytes_, express_batch_bytes_);
-                for (auto it = queue_.begin(); it != queue_.end();) {
-                    ServeReq* r = reqs_.at(*it).get();
-                    if (r->dc != dc || r->width != width || !admissible(k, *r)) {  // left for another lane
-                        ++it;
-                        continue;
-                    }
-                    if (!batch.empty() && (text_bytes + r->n > cap || batch.size() >= batch_texts_))
-                        break;
-                    if (reserved_ + r->footprint > budget_) break;  // first come, first served
-                    reserved_ += r->footprint;
-                    scratch += r->footprint - serve_result_bytes(r->n, width);
-                    text_bytes += r->n;
-                    r->status = 1;
-                    r->lane = k;
-                    r->t_start = std::chrono::steady_clock::now();
-                    batch.push_back(r);
-                    it = queue_.erase(it);
-                }
-                running_++;
-                st_.batches++;
-                st_.peak_reserved_bytes = std::max<uint64_t>(st_.peak_reserved_bytes, reserved_);
-                st_.max_batch_texts = std::max<uint64_t>(st_.max_batch_texts, batch.size());
+            if (cur.empty()) {
+                if (!admit(k, true, cur)) break;
+                if (cur.empty()) continue;
+                upload(k, cur);
             }
-            cv_work_.notify_all();  // the rest of the queue may fit another lane
+            if (k == 0) {
+                if (!admit(k, false, nxt)) {
+                    nxt = Batch{};
+                }
+                if (!nxt.empty()) upload(k, nxt);
+            }
             int err = DCX_OK;
             std::shared_ptr<ServeResult> res;
-            std::vector<uint64_t> offs(batch.size() + 1, 0);
             try {
-                res = run(c, batch, scratch, offs);
+                res = build(k, cur);
             } catch (const Error& e) {
                 err = e.code;
+                res.reset();
             } catch (...) {
                 err = DCX_ERR_INTERNAL;
+                res.reset();
             }
-            {
-                std::lock_guard<std::mutex> lk(mu_);
-                const auto now = std::chrono::steady_clock::now();
-                uint64_t result_bytes = 0;
-                for (size_t i = 0; i < batch.size(); i++) {
-                    ServeReq* r = batch[i];
-                    r->t_done = now;
-                    r->text.reset();
-                    r->borrowed = nullptr;
-                    if (r->pinned) {
-                        arena_.free(r->pinned);
-                        r->pinned = nullptr;
-                    }
-                    if (err == DCX_OK) {
-                        r->status = 2;
-                        r->res = res;
-                        r->res_off = offs[i] * (uint64_t)(r->width / 8);
-                        st_.done++;
-                        st_.done_bytes += r->n;
-                    } else {
-                        r->status = err;
-                        st_.failed++;
-                    }
-                }
-                if (err == DCX_OK && res) {
-                    res->refs = (uint32_t)batch.size();
-                    result_bytes = res->bytes;
-                }
-                // the scratch and text parts end with the batch, the result stays until released
-                uint64_t fp = 0;
-                for (ServeReq* r : batch) fp += r->footprint;
-                reserved_ -= fp - result_bytes;
-                st_.peak_lane_bytes = std::max<uint64_t>(st_.peak_lane_bytes, c.peak);
-                running_--;
-            }
-            cv_work_.notify_all();
-            cv_done_.notify_all();
+            drop_upload(k, cur);
+            complete(k, cur, res, err);
+            cur = std::move(nxt);
+            nxt = Batch{};
         }
+        // stopping: a prefetched batch is abandoned (its requests are dropped with the server)
+        if (!cur.empty()) drop_upload(k, cur);
+        cudaStreamSynchronize(lanes_[k]->stream);
     }
 
     static const uint8_t* text_of(const ServeReq& r) {
         if (r.borrowed) return r.borrowed;
         if (r.pinned) return r.pinned;
         return r.text.get();
-    }
-
-    // Uploads the batch's texts, builds their SAs into one device buffer.
-    std::shared_ptr<ServeResult> run(Ctx& c, const std::vector<ServeReq*>& batch, uint64_t scratch,
-                                     std::vector<uint64_t>& offs) {
-        const int width = batch[0]->width, dc = batch[0]->dc;
-        for (size_t i = 0; i < batch.size(); i++) offs[i + 1] = offs[i] + batch[i]->n;
-        const uint64_t total = offs.back();
-        auto res = std::make_shared<ServeResult>();
-        res->stream = c.stream;
-        res->bytes = serve_result_bytes(total, width);
-        void* d_text = nullptr;
-        DCX_CUDA(cudaMallocFromPoolAsync(&d_text, total + 16, c.pool, c.stream));
-        if (cudaMallocFromPoolAsync(&res->p, res->bytes, c.pool, c.stream) != cudaSuccess) {
-            cudaGetLastError();
-            cudaFreeAsync(d_text, c.stream);
-            throw Error(DCX_ERR_OOM, "result buffer");
-        }
-        cudaEvent_t ev[3];
-        for (auto& e : ev) cudaEventCreate(&e);
-        cudaEventRecord(ev[0], c.stream);
-        try {
-            for (size_t i = 0; i < batch.size(); i++)
-                if (batch[i]->n)
-                    DCX_CUDA(cudaMemcpyAsync((uint8_t*)d_text + offs[i], text_of(*batch[i]), batch[i]->n,
-                                             batch[i]->borrowed_dev ? cudaMemcpyDeviceToDevice
-                                                                    : cudaMemcpyHostToDevice,
-                                             c.stream));
-            cudaEventRecord(ev[1], c.stream);
-            c.budget = c.in_use + scratch;  // build_batch sizes its rounds from this
-            build_batch(c, (const uint8_t*)d_text, offs.data(), (uint32_t)batch.size(), dc, width, res->p,
-                        DCX_DEVICE_PTRS);
-            cudaEventRecord(ev[2], c.stream);
-            DCX_CUDA(cudaStreamSynchronize(c.stream));
-        } catch (...) {
-            cudaFreeAsync(d_text, c.stream);
-            for (auto& e : ev) cudaEventDestroy(e);
-            throw;
-        }
-        float up = 0, bd = 0;
-        cudaEventElapsedTime(&up, ev[0], ev[1]);
-        cudaEventElapsedTime(&bd, ev[1], ev[2]);
-        for (auto& e : ev) cudaEventDestroy(e);
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            st_.ms_upload += up;
-            st_.ms_build += bd;
-        }
-        DCX_CUDA(cudaFreeAsync(d_text, c.stream));
-        return res;
     }
 
     int device_;
@@ -498,6 +579,7 @@ private:
     bool stop_ = false;
     dcx_serve_stats st_{};
     std::vector<std::unique_ptr<Ctx>> lanes_;
+    std::vector<cudaStream_t> copy_streams_;  // per lane: uploads of the texts
     std::vector<std::thread> threads_;
     cudaStream_t copy_stream_ = nullptr;
 };

@@ -166,14 +166,16 @@ typedef struct dcx_serve_stats {
  * DCX_ERR_BUDGET if its projected footprint can never fit the budget.  The
  * serving budget is the option "serve_budget" (bytes; 0 = the context budget),
  * read when the first request starts the server, as are "serve_lanes"
- * (default 2), "serve_batch_bytes" (text bytes per batch, default 1 GiB) and
+ * (default 1), "serve_batch_bytes" (text bytes per batch, default 1 GiB) and
  * "serve_batch_texts" (requests per batch, default 65536),
  * "serve_host_bytes" (pinned host memory for request copies, default 8 GiB;
  * requests that do not fit it are copied to pageable memory) and
- * "serve_express_bytes" (default 4 MiB): lane 0 serves every request in
- * arrival order, the other lanes (on high-priority streams) only requests up
- * to this length, in batches of at most 4x it, so long builds run one at a
- * time and short requests do not wait behind them. */
+ * "serve_express_bytes" (default 4 MiB): lane 0 serves the requests longer
+ * than this (all requests when it is the only lane), uploading its next batch
+ * while it builds the current one; the other lanes, on high-priority streams,
+ * serve the shorter ones in batches of at most 4x it.  Each class is served in
+ * arrival order, long builds run one at a time and short requests do not wait
+ * behind them. */
 int dcx_serve_submit(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
                      uint64_t* req_id);
 /* dcx_serve_submit with flags: DCX_SERVE_BORROW skips the copy at submission --
