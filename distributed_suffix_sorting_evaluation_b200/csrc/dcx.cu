@@ -616,6 +616,29 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         for (uint32_t w = 0; w < kwr; w++) ko.w[w] = s.k[0][w];
         const int grid = grid_for(cnt, 256, 148 * 8);
         const size_t shm = (size_t)HIST_COPIES * 4 * kwr * RADIX * 4;
+        const bool swar = sizeof(CharT) == 1 && B <= 256 && Pr <= 64 && ((uintptr_t)text & 7) == 0;
+        if (swar) {
+            // byte text: aligned word loads + SWAR digit folding
+            RefinePlan8 r8{};
+            r8.P = Pr;
+            r8.m = (Pr + 7) / 8;
+            r8.r = Pr - 8 * (r8.m - 1);
+            r8.B = B;
+            r8.B2 = B * B;
+            r8.B4 = r8.B2 * r8.B2;
+            r8.pow8 = r8.B4 * r8.B4;  // only used when m > 1, i.e. B^8 < 2^64
+            r8.powr = 1;
+            for (uint32_t i = 0; i < r8.r; i++) r8.powr *= B;
+            const uint8_t* t8 = reinterpret_cast<const uint8_t*>(text);
+            DCX_CUDA(cudaFuncSetAttribute(k_keys_refine8<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+            DCX_CUDA(cudaFuncSetAttribute(k_keys_refine8<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
+            if (rp.kw == 1)
+                k_keys_refine8<1><<<grid, 256, shm, c.stream>>>(t8, sv, cnt, tpos.get(), SEGK ? tseg.get() : nullptr,
+                                                                 grp.get(), covered, r8, ko, s.v[0], c.d_hist);
+            else
+                k_keys_refine8<2><<<grid, 256, shm, c.stream>>>(t8, sv, cnt, tpos.get(), SEGK ? tseg.get() : nullptr,
+                                                                 grp.get(), covered, r8, ko, s.v[0], c.d_hist);
+        } else {
         DCX_CUDA(cudaFuncSetAttribute(k_keys_refine<1, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
         DCX_CUDA(cudaFuncSetAttribute(k_keys_refine<2, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
         if (rp.kw == 1)
@@ -624,6 +647,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         else
             k_keys_refine<2, CharT><<<grid, 256, shm, c.stream>>>(text, sv, cnt, tpos.get(), SEGK ? tseg.get() : nullptr,
                                                                   grp.get(), covered, rp, ko, s.v[0], c.d_hist);
+        }
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(cnt * (12 + Pr * sizeof(CharT)) + cnt * (kwr + 1) * 4);
@@ -644,7 +668,8 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
 // ---------------------------------------------------------------------------
 template <int D>
 static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_text, const DcDev* dcd, TieSeg ts,
-                        const std::vector<uint32_t>& counts, const uint32_t* gstart, const uint32_t* gsize) {
+                        const std::vector<uint32_t>& counts, const uint32_t* gstart, const uint32_t* gsize,
+                        uint32_t X) {
     std::vector<uint64_t> off(TIE_CLASSES + 1, 0);
     for (int k = 0; k < TIE_CLASSES; k++) off[k + 1] = off[k] + counts[k];
     auto warp_launch = [&](int cls, auto W) {
@@ -667,14 +692,14 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         constexpr int C = decltype(Cc)::value;
         constexpr int T = C / 2 < 512 ? C / 2 : 512;
         if (!g) return;
-        const size_t shm = tie_cta_smem<D, C>();
+        const size_t shm = tie_cta_smem<D, C>(X);
         DCX_CUDA(cudaFuncSetAttribute(k_tie_cta<D, C, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        for (uint64_t b = 0; b < g; b += 65535ull * 1024) {
-            const uint64_t nb = std::min<uint64_t>(g - b, 65535ull * 1024);
-            k_tie_cta<D, C, T><<<(unsigned)nb, T, shm, c.stream>>>(gs + b, gz + b, sa, rank_text, dcd, ts);
-            DCX_CHECK_LAUNCH();
-            c.launched();
-        }
+        int per_sm = 0;  // CTAs that fit one SM: the grid loops over the groups
+        DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tie_cta<D, C, T>, T, shm));
+        const uint64_t grid = std::min<uint64_t>(g, 148ull * std::max(per_sm, 1));
+        k_tie_cta<D, C, T><<<(unsigned)grid, T, shm, c.stream>>>(gs, gz, g, sa, rank_text, dcd, ts);
+        DCX_CHECK_LAUNCH();
+        c.launched();
     };
     cta_launch(gstart + off[5], gsize + off[5], counts[5], std::integral_constant<int, 64>{});
     cta_launch(gstart + off[6], gsize + off[6], counts[6], std::integral_constant<int, 128>{});
@@ -754,7 +779,7 @@ static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, con
     const DcDev* dcd = c.dc_dev[dc.X];
     switch (dc.D) {
 #define DCX_TIE(DV) \
-    case DV: tie_break_d<DV>(c, sa, N, rank_text, dcd, ts, counts, gstart.get(), gsize.get()); break;
+    case DV: tie_break_d<DV>(c, sa, N, rank_text, dcd, ts, counts, gstart.get(), gsize.get(), dc.X); break;
         DCX_TIE(2) DCX_TIE(3) DCX_TIE(4) DCX_TIE(5) DCX_TIE(6) DCX_TIE(7) DCX_TIE(8) DCX_TIE(9) DCX_TIE(10)
         DCX_TIE(11) DCX_TIE(12)
 #undef DCX_TIE

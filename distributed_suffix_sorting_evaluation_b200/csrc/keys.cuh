@@ -280,4 +280,67 @@ __global__ __launch_bounds__(256) void k_keys_refine(const CharT* __restrict__ t
     hist_flush(sh, 4 * (KW + 1) * RADIX, hist);
 }
 
+// Refinement keys of byte texts (base B <= 256, window P <= 64 chars, key < 2^64).
+// The window [s, s+P) is read as aligned 8-byte words (independent loads, at
+// most 9), funnel-shifted so that word k holds window chars 8k..8k+7, and each
+// word is folded into its base-B value with three SWAR multiply-adds (pairs,
+// quads, octets; no lane overflows for B <= 256).  Chars at or past the text's
+// end count as 0.  The integer equals the one encode_window builds.
+struct RefinePlan8 {
+    uint32_t P, m, r;          // chars, words (ceil(P/8)), chars in the last word
+    uint64_t B, B2, B4;        // B, B^2, B^4
+    uint64_t pow8, powr;       // B^8, B^r
+};
+
+__device__ __forceinline__ uint64_t swar_digits8(uint64_t w, const RefinePlan8& rp) {
+    // byte 0 is the most significant digit
+    const uint64_t t16 = (w & 0x00ff00ff00ff00ffull) * rp.B + ((w >> 8) & 0x00ff00ff00ff00ffull);
+    const uint64_t t32 = (t16 & 0x0000ffff0000ffffull) * rp.B2 + ((t16 >> 16) & 0x0000ffff0000ffffull);
+    return (t32 & 0xffffffffull) * rp.B4 + (t32 >> 32);
+}
+
+template <int KW>
+__global__ __launch_bounds__(256) void k_keys_refine8(const uint8_t* __restrict__ text, SegView sv, uint64_t count,
+                                                      const uint32_t* __restrict__ tpos,
+                                                      const uint32_t* __restrict__ tseg,
+                                                      const uint32_t* __restrict__ grp, uint32_t off, RefinePlan8 rp,
+                                                      KeyOut ko, uint32_t* __restrict__ vals_out, uint32_t* hist) {
+    extern __shared__ uint32_t sh[];  // HIST_COPIES * 4*(KW+1) * RADIX
+    hist_zero(sh, 4 * (KW + 1) * RADIX);
+    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < count;
+         j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t pos = tpos[j];
+        const uint64_t end = seg_end(sv, tseg ? tseg[j] : 0u);
+        const uint64_t s = (uint64_t)pos + off;
+        const uint64_t a0 = s & ~7ull;
+        const uint32_t shb = (uint32_t)(s - a0) * 8u;
+        uint64_t w[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++)  // words at or past the end hold only zero chars: not read
+            w[k] = ((uint32_t)k <= rp.m && a0 + 8ull * k < end) ? __ldg(tw0 + (a0 >> 3) + k) : 0ull;
+        const uint64_t v = end > s ? end - s : 0;  // window chars inside the text
+        uint64_t key = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if ((uint32_t)k >= rp.m) break;
+            uint64_t cw = shb ? (w[k] >> shb) | (w[k + 1] << (64u - shb)) : w[k];
+            const int64_t vk = (int64_t)v - 8 * k;
+            if (vk < 8) cw = vk <= 0 ? 0ull : cw & ((1ull << (8 * vk)) - 1ull);
+            const bool last = (uint32_t)k == rp.m - 1;
+            if (last && rp.r < 8) cw <<= 8u * (8u - rp.r);  // drop chars past the window; keep r low digits
+            key = key * (last ? rp.powr : rp.pow8) + swar_digits8(cw, rp);
+        }
+        uint32_t kk[KW + 1];
+        kk[0] = (uint32_t)key;
+        if (KW > 1) kk[1] = (uint32_t)(key >> 32);
+        kk[KW] = grp[j];
+#pragma unroll
+        for (int w2 = 0; w2 <= KW; w2++) ko.w[w2][j] = kk[w2];
+        vals_out[j] = pos;
+        hist_add<KW + 1>(sh, kk);
+    }
+    hist_flush(sh, 4 * (KW + 1) * RADIX, hist);
+}
+
 }  // namespace dcx

@@ -141,45 +141,74 @@ __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ g
     if (valid) sa[start + l] = (uint32_t)(a.pos + pos0);
 }
 
-// One group (or chunk) of up to C elements per CTA; bitonic network in shared memory.
+// Groups (or chunks) of up to C elements, one at a time per CTA (the CTA loops
+// over groups, so the comparator table is loaded once).  The group's records
+// stay in place in shared memory as structure of arrays (position, residue mod
+// X, D cover ranks); a bitonic network permutes 16-bit indices, and each
+// comparison reads just the two ranks it needs.
 template <int D, int C, int THREADS>
 __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize,
-                                                     uint32_t* __restrict__ sa, const uint32_t* __restrict__ rank_text,
+                                                     uint64_t ngroups, uint32_t* __restrict__ sa,
+                                                     const uint32_t* __restrict__ rank_text,
                                                      const DcDev* __restrict__ dcp, TieSeg ts) {
-    extern __shared__ uint32_t smem[];
-    uint16_t* tab = reinterpret_cast<uint16_t*>(smem);
-    uint32_t* nr = smem + (MAX_X * MAX_X + 1) / 2;
-    Rec<D>* recs = reinterpret_cast<Rec<D>*>(nr + MAX_X);
-    load_dc_smem(*dcp, tab, nr);
+    static_assert(C <= 65536, "indices are 16-bit");
+    extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t X = dcp->X;
-    const uint32_t start = gstart[blockIdx.x], size = gsize[blockIdx.x];
-    uint64_t pos0, slot0;
-    tie_bases(ts, start, pos0, slot0);
-    for (uint32_t i = threadIdx.x; i < C; i += THREADS)
-        recs[i] = load_rec<D>(i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS, rank_text + slot0, X, nr);
-    __syncthreads();
-    for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t p = threadIdx.x; p < (uint32_t)C / 2; p += THREADS) {
-                const uint32_t i = 2 * j * (p / j) + (p % j);
-                const uint32_t q = i + j;
-                const bool up = (i & k) == 0;
-                Rec<D> a = recs[i], b = recs[q];
-                const bool swap = up ? dc_less<D>(b, a, X, tab) : dc_less<D>(a, b, X, tab);
-                if (swap) {
-                    recs[i] = b;
-                    recs[q] = a;
-                }
-            }
-            __syncthreads();
+    uint32_t* s_pos = smem;                                         // [C]
+    uint32_t* s_rk = s_pos + C;                                     // [C * D]
+    uint32_t* nr = s_rk + C * D;                                    // [MAX_X]
+    uint16_t* s_idx = reinterpret_cast<uint16_t*>(nr + MAX_X);      // [C]
+    uint16_t* tab = s_idx + C;                                      // [X * X]
+    uint8_t* s_res = reinterpret_cast<uint8_t*>(tab + X * X);       // [C]
+    load_dc_smem(*dcp, tab, nr);
+    auto less = [&](uint32_t ia, uint32_t ib) -> bool {
+        const uint32_t pa = s_pos[ia], pb = s_pos[ib];
+        if (pa == INVALID_POS) return false;
+        if (pb == INVALID_POS) return true;
+        const uint16_t e = tab[s_res[ia] * X + s_res[ib]];
+        return s_rk[ia * D + (e & 0xffu)] < s_rk[ib * D + (e >> 8)];
+    };
+    for (uint64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const uint32_t start = gstart[g], size = gsize[g];
+        uint64_t pos0, slot0;
+        tie_bases(ts, start, pos0, slot0);
+        for (uint32_t i = threadIdx.x; i < (uint32_t)C; i += THREADS) {
+            const uint32_t p = i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS;
+            s_pos[i] = p;
+            s_res[i] = p == INVALID_POS ? 0 : (uint8_t)(p % X);
+            s_idx[i] = (uint16_t)i;
         }
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < size * D; t += THREADS) {  // ranks, D consecutive words per element
+            const uint32_t i = t / D, k = t - i * D;
+            const uint32_t p = s_pos[i];
+            s_rk[t] = __ldg(rank_text + slot0 + (uint64_t)(p / X) * D + nr[s_res[i]] + k);
+        }
+        __syncthreads();
+        for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t p = threadIdx.x; p < (uint32_t)C / 2; p += THREADS) {
+                    const uint32_t i = 2 * j * (p / j) + (p % j);
+                    const uint32_t q = i + j;
+                    const bool up = (i & k) == 0;
+                    const uint32_t a = s_idx[i], b = s_idx[q];
+                    const bool swap = up ? less(b, a) : less(a, b);
+                    if (swap) {
+                        s_idx[i] = (uint16_t)b;
+                        s_idx[q] = (uint16_t)a;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t i = threadIdx.x; i < size; i += THREADS) sa[start + i] = (uint32_t)(s_pos[s_idx[i]] + pos0);
+        __syncthreads();  // shared arrays are reused by the next group
     }
-    for (uint32_t i = threadIdx.x; i < size; i += THREADS) sa[start + i] = (uint32_t)(recs[i].pos + pos0);
 }
 
 template <int D, int C>
-constexpr size_t tie_cta_smem() {
-    return sizeof(uint32_t) * ((MAX_X * MAX_X + 1) / 2 + MAX_X) + sizeof(Rec<D>) * C;
+inline size_t tie_cta_smem(uint32_t X) {
+    return sizeof(uint32_t) * ((size_t)C * (1 + D) + MAX_X) + sizeof(uint16_t) * ((size_t)C + (size_t)X * X) + C + 16;
 }
 
 // One merge round for groups larger than a chunk.  Flat element f belongs to

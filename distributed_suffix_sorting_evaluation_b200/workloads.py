@@ -88,6 +88,13 @@ def batch_lengths(count: int, lmin: int = 1 << 10, lmax: int = 16 << 20, seed: i
     return out
 
 
+DESCRIPTIONS = {
+    "cfg1_dc3_iid_dna_64MiB": "synthetic (seeded i.i.d. uniform {A,C,G,T})",
+    "cfg2_dc39_markov_dna_1GiB": "synthetic (seeded order-3 Markov DNA + 5% repeats; no public corpus)",
+    "cfg3a_dc39_pangenome_2GiB": "synthetic (200 mutated copies of a seeded 10 MiB {A,C,G,T} base, '$'-separated)",
+    "cfg3b_dc39_zipf256_1GiB": "synthetic (seeded Zipf(s=1.1) over 256 byte values)",
+}
+
 WORKLOADS = {
     "cfg1_dc3_iid_dna_64MiB": dict(gen="iid_dna", n=64 << 20, dc=3, sa_width=64, seed=1),
     "cfg2_dc39_markov_dna_1GiB": dict(gen="markov_dna", n=1 << 30, dc=39, sa_width=40, seed=2),
