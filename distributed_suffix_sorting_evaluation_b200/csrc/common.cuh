@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "dcx_gpu.h"
 
@@ -107,18 +108,38 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
+// An operator may also supply   void load16(uint64_t base, uint64_t n, T* v)
+// (the 16 values of elements base..base+15, zero past n; base is a multiple of
+// 16), which it implements with vector loads; both scan phases then give each
+// thread 16 consecutive elements.
+template <typename Op, typename = void>
+struct ScanVec : std::false_type {};
+template <typename Op>
+struct ScanVec<Op, std::void_t<decltype(&Op::load16)>> : std::true_type {};
+
 // Loads are warp-striped: lane l of warp w reads element w*32*ITEMS + it*32 + l
 // of the tile in iteration it, so every load instruction is coalesced.
 template <typename T, typename Op>
 __global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(Op op, uint64_t n, T* tile_sums) {
     __shared__ T sm[SCAN_THREADS / 32 + 1];
-    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)(threadIdx.x >> 5) * 32 * SCAN_ITEMS +
-                          (threadIdx.x & 31);
     T acc = T(0);
+    if constexpr (ScanVec<Op>::value) {
+        static_assert(SCAN_ITEMS == 16, "load16 covers a thread's items");
+        const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+        if (base < n) {
+            T v[16];
+            op.load16(base, n, v);
 #pragma unroll
-    for (int it = 0; it < SCAN_ITEMS; it++) {
-        const uint64_t i = base + (uint64_t)it * 32;
-        if (i < n) acc += op.load(i);
+            for (int it = 0; it < 16; it++) acc += v[it];
+        }
+    } else {
+        const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)(threadIdx.x >> 5) * 32 * SCAN_ITEMS +
+                              (threadIdx.x & 31);
+#pragma unroll
+        for (int it = 0; it < SCAN_ITEMS; it++) {
+            const uint64_t i = base + (uint64_t)it * 32;
+            if (i < n) acc += op.load(i);
+        }
     }
     T total;
     block_excl_scan<SCAN_THREADS>(acc, sm, total);
@@ -149,11 +170,22 @@ __global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(Op op, uint64_t n, 
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
     T vals[SCAN_ITEMS];
     T acc = T(0);
+    if constexpr (ScanVec<Op>::value) {
+        if (base < n) {
+            op.load16(base, n, vals);
+        } else {
 #pragma unroll
-    for (int it = 0; it < SCAN_ITEMS; it++) {
-        const uint64_t i = base + it;
-        vals[it] = i < n ? op.load(i) : T(0);
-        acc += vals[it];
+            for (int it = 0; it < SCAN_ITEMS; it++) vals[it] = T(0);
+        }
+#pragma unroll
+        for (int it = 0; it < SCAN_ITEMS; it++) acc += vals[it];
+    } else {
+#pragma unroll
+        for (int it = 0; it < SCAN_ITEMS; it++) {
+            const uint64_t i = base + it;
+            vals[it] = i < n ? op.load(i) : T(0);
+            acc += vals[it];
+        }
     }
     T total;
     const T ex = block_excl_scan<SCAN_THREADS>(acc, sm, total);
@@ -178,6 +210,47 @@ __device__ __forceinline__ void store_sa_entry(void* out, uint64_t k, uint32_t v
         o[3] = (uint8_t)(v >> 24);
         o[4] = 0;
     }
+}
+
+// Unsigned 32-bit division by a divisor fixed per launch (Granlund and
+// Montgomery's round-up method): with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, q = (umulhi(m, a) + a) >> l for every
+// 32-bit a (the sum is formed in 64 bits).  A runtime-divisor '%' or '/' costs
+// a few dozen instructions; this costs four.
+struct FastDiv {
+    uint32_t d, m, l;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f{d, 0, 0};
+    while ((1ull << f.l) < d) f.l++;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << f.l) - d)) / d) + 1);
+    return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t a, const FastDiv& f) {
+    return (uint32_t)(((uint64_t)__umulhi(f.m, a) + a) >> f.l);
+}
+__device__ __forceinline__ void fdivmod(uint32_t a, const FastDiv& f, uint32_t& q, uint32_t& r) {
+    q = fdiv(a, f);
+    r = a - q * f.d;
+}
+
+// 16 flag bytes f[base..base+15] plus f[base+16] (`past` when base+16 >= n);
+// base is a multiple of 16 and the array is 16-byte aligned.  Bytes at or past
+// n read as `past`.
+__device__ __forceinline__ void load_flags17(const uint8_t* __restrict__ f, uint64_t base, uint64_t n, uint32_t past,
+                                             uint32_t* b) {
+    if (base + 16 <= n) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(f + base));
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 16; k++) b[k] = (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) b[k] = base + k < n ? f[base + k] : past;
+    }
+    b[16] = base + 16 < n ? f[base + 16] : past;
 }
 
 }  // namespace dcx

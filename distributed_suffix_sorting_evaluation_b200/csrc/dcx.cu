@@ -349,6 +349,7 @@ static const DcHost& get_dc(Ctx& c, uint32_t X) {
     if (!make_dc(X, h)) throw Error(DCX_ERR_ARG, "unsupported difference cover X=" + std::to_string(X));
     DcDev dd{};
     dd.X = X;
+    dd.fx = make_fastdiv(X);
     dd.D = h.D;
     for (uint32_t i = 0; i < X; i++) dd.next_rank[i] = h.next_rank[i];
     for (uint32_t i = 0; i < h.D; i++) dd.dc[i] = h.dc[i];
@@ -501,11 +502,11 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     uint32_t P0 = std::min<uint32_t>(L, max_chars_in_bits_k(B, 32 * std::min(words_full, kw0_max), K));
     if (depth == 0 && c.level0_entropy > 0.05) {
         // Shortest byte-aligned prefix whose expected random collisions stay near
-        // 1% of N: P * H >= log2(N) + 7, with H the order-0 entropy discounted by
-        // 15% for context dependence.  Ties left over are resolved exactly by the
+        // 1% of N: P * H >= log2(N) + 6, with H the order-0 entropy discounted by
+        // 5% for context dependence.  Ties left over are resolved exactly by the
         // refinement rounds, so this only trades passes against refinement work.
-        const double need = std::log2((double)N) + 7.0;
-        uint32_t P = (uint32_t)std::ceil(need / (0.85 * c.level0_entropy));
+        const double need = std::log2((double)N) + 6.0;
+        uint32_t P = (uint32_t)std::ceil(need / (0.95 * c.level0_entropy));
         P = std::max<uint32_t>(1, std::min(P, P0));
         const uint32_t bytes = (key_bits_k(B, P, K) + 7) / 8;
         const uint32_t fill = std::min<uint32_t>(P0, max_chars_in_bits_k(B, 8 * bytes, K));
@@ -683,7 +684,12 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         DCX_CHECK_LAUNCH();
         c.launched();
     };
-    warp_launch(0, std::integral_constant<int, 2>{});
+    if (counts[0]) {  // pairs
+        k_tie_pair<<<grid_for(counts[0], 256, 148 * 16), 256, 0, c.stream>>>(gstart + off[0], counts[0], sa, rank_text,
+                                                                           dcd, ts);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    }
     warp_launch(1, std::integral_constant<int, 4>{});
     warp_launch(2, std::integral_constant<int, 8>{});
     warp_launch(3, std::integral_constant<int, 16>{});
@@ -874,6 +880,7 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
     DcFlags fl{};
     fl.X = X;
     fl.D = D;
+    fl.fx = make_fastdiv(X);
     for (uint32_t i = 0; i < X; i++) {
         fl.in_dc[i] = dc.in_dc[i];
         fl.next_rank[i] = dc.next_rank[i];

@@ -17,6 +17,7 @@ namespace dcx {
 
 struct DcFlags {
     uint32_t X, D;
+    FastDiv fx;  // division by X
     uint8_t in_dc[MAX_X];
     uint32_t next_rank[MAX_X];
     uint32_t dc[MAX_D];
@@ -48,7 +49,9 @@ __device__ __forceinline__ uint32_t bsearch_le(const uint64_t* a, uint32_t K, ui
 }
 
 __device__ __forceinline__ uint64_t slot_of_local(uint64_t i, const DcFlags& f) {
-    return (i / f.X) * f.D + f.next_rank[i % f.X];
+    uint32_t q, r;
+    fdivmod((uint32_t)i, f.fx, q, r);  // positions are < 2^32
+    return (uint64_t)q * f.D + f.next_rank[r];
 }
 
 // ---- alphabet (cli.cpp:417-463) ---------------------------------------------
@@ -183,6 +186,13 @@ struct OpTied {
         const uint32_t tied = !(h && nh);
         return (uint64_t)h | ((uint64_t)tied << 32);
     }
+    __device__ void load16(uint64_t base, uint64_t n, uint64_t* v) const {
+        uint32_t b[17];
+        load_flags17(head, base, N, 1u, b);
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            v[k] = base + k < n ? ((uint64_t)b[k] | ((uint64_t)!(b[k] && b[k + 1]) << 32)) : 0ull;
+    }
     __device__ void store(uint64_t k, uint64_t ex, uint64_t v) const {
         if (v >> 32) {
             const uint32_t j = (uint32_t)(ex >> 32);
@@ -227,8 +237,41 @@ struct OpSamples {
     __device__ uint64_t load(uint64_t k) const {
         const uint32_t sg = segw ? segw[k] : 0u;
         const uint64_t i = sa[k] - ls.start[sg];
-        const uint32_t smp = f->in_dc[i % f->X];
+        uint32_t q, r;
+        fdivmod((uint32_t)i, f->fx, q, r);
+        const uint32_t smp = f->in_dc[r];
         return (uint64_t)head[k] | ((uint64_t)smp << 32);
+    }
+    __device__ void load16(uint64_t base, uint64_t n, uint64_t* v) const {
+        uint32_t b[17];
+        load_flags17(head, base, n, 0u, b);
+        uint32_t p[16];
+        if (base + 16 <= n) {  // sa (and segw) are 16-byte aligned device arrays
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint4 q4 = __ldg(reinterpret_cast<const uint4*>(sa + base) + k);
+                p[4 * k] = q4.x; p[4 * k + 1] = q4.y; p[4 * k + 2] = q4.z; p[4 * k + 3] = q4.w;
+            }
+            if (segw) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const uint4 s4 = __ldg(reinterpret_cast<const uint4*>(segw + base) + k);
+                    p[4 * k] -= (uint32_t)ls.start[s4.x]; p[4 * k + 1] -= (uint32_t)ls.start[s4.y];
+                    p[4 * k + 2] -= (uint32_t)ls.start[s4.z]; p[4 * k + 3] -= (uint32_t)ls.start[s4.w];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++)
+                p[k] = base + k < n ? (uint32_t)(sa[base + k] - ls.start[segw ? segw[base + k] : 0u]) : 0u;
+        }
+        const FastDiv fx = f->fx;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            uint32_t q, r;
+            fdivmod(p[k], fx, q, r);
+            v[k] = base + k < n ? ((uint64_t)b[k] | ((uint64_t)f->in_dc[r] << 32)) : 0ull;
+        }
     }
     __device__ void store(uint64_t k, uint64_t ex, uint64_t v) const {
         if (v >> 32) {
@@ -458,6 +501,13 @@ struct OpGroups {
         const uint32_t s = h && !nh;
         const uint32_t e = !h && nh;
         return (uint64_t)s | ((uint64_t)e << 32);
+    }
+    __device__ void load16(uint64_t base, uint64_t n, uint64_t* v) const {
+        uint32_t b[17];
+        load_flags17(head, base, N, 1u, b);
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            v[k] = base + k < n ? ((uint64_t)(b[k] && !b[k + 1]) | ((uint64_t)(!b[k] && b[k + 1]) << 32)) : 0ull;
     }
     __device__ void store(uint64_t k, uint64_t ex, uint64_t v) const {
         if (v & 0xffffffffull) starts[(uint32_t)ex] = (uint32_t)k;

@@ -58,12 +58,14 @@ struct SortPassArgs {
     uint32_t spin_limit;
 };
 
-// Lanes of the warp holding the same 8-bit digit (plus a validity bit), from
-// nine ballots; stable ranking needs only the lanes below this one.
+// Lanes of the warp holding the same 8-bit digit, from eight ballots, or nine
+// when some lanes hold no element (digit RADIX); stable ranking needs only the
+// lanes below this one.
+template <bool PARTIAL>
 __device__ __forceinline__ uint32_t warp_digit_peers(uint32_t d) {
     uint32_t peers = 0xffffffffu;
 #pragma unroll
-    for (int b = 0; b < RADIX_BITS + 1; b++) {
+    for (int b = 0; b < RADIX_BITS + (PARTIAL ? 1 : 0); b++) {
         const uint32_t bit = (d >> b) & 1u;
         const uint32_t bal = __ballot_sync(0xffffffffu, bit);
         peers &= bit ? bal : ~bal;
@@ -169,10 +171,11 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
     }
     // 2. stable rank inside the warp, positions in the sorted tile
     uint32_t pos[ITEMS];
+    const bool full = tile_valid == (uint32_t)TILE;
 #pragma unroll
     for (int it = 0; it < ITEMS; it++) {
         const uint32_t d = dig[it];
-        const uint32_t peers = warp_digit_peers(d);
+        const uint32_t peers = full ? warp_digit_peers<false>(d) : warp_digit_peers<true>(d);
         const uint32_t before = __popc(peers & lanemask_lt());
         uint32_t base = 0;
         if (d < RADIX) base = s_warp_hist[warp][d];

@@ -25,6 +25,7 @@ constexpr uint32_t INVALID_POS = 0xffffffffu;
 
 struct DcDev {
     uint32_t X, D;
+    FastDiv fx;  // division by X
     uint32_t next_rank[MAX_X];
     uint32_t dc[MAX_D];
     uint16_t cmp[MAX_X * MAX_X];  // r1 | r2 << 8
@@ -61,7 +62,8 @@ __device__ __forceinline__ Rec<D> load_rec(uint32_t pos, const uint32_t* __restr
         for (int k = 0; k < D; k++) r.r[k] = 0;
         return r;
     }
-    const uint64_t rp = (uint64_t)(pos / X) * D + next_rank[pos % X];
+    const uint32_t q = pos / X;
+    const uint64_t rp = (uint64_t)q * D + next_rank[pos - q * X];
 #pragma unroll
     for (int k = 0; k < D; k++) r.r[k] = __ldg(rank_text + rp + k);
     return r;
@@ -99,6 +101,35 @@ __device__ __forceinline__ void load_dc_smem(const DcDev& dc, uint16_t* tab, uin
     for (uint32_t i = threadIdx.x; i < XX; i += blockDim.x) tab[i] = dc.cmp[i];
     for (uint32_t i = threadIdx.x; i < dc.X; i += blockDim.x) nr[i] = dc.next_rank[i];
     __syncthreads();
+}
+
+// Groups of exactly two elements, one per thread: the comparator needs one
+// cover rank of each suffix, so only those two ranks are read.
+__global__ __launch_bounds__(256) void k_tie_pair(const uint32_t* __restrict__ gstart, uint64_t ngroups,
+                                                  uint32_t* __restrict__ sa, const uint32_t* __restrict__ rank_text,
+                                                  const DcDev* __restrict__ dcp, TieSeg ts) {
+    __shared__ uint16_t tab[MAX_X * MAX_X];
+    __shared__ uint32_t nr[MAX_X];
+    load_dc_smem(*dcp, tab, nr);
+    const uint32_t X = dcp->X, D = dcp->D;
+    const FastDiv fx = dcp->fx;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t start = gstart[g];
+        uint64_t pos0, slot0;
+        tie_bases(ts, start, pos0, slot0);
+        const uint32_t a = (uint32_t)(sa[start] - pos0), b = (uint32_t)(sa[start + 1] - pos0);
+        uint32_t qa, ma, qb, mb;
+        fdivmod(a, fx, qa, ma);
+        fdivmod(b, fx, qb, mb);
+        const uint16_t e = tab[ma * X + mb];
+        const uint32_t ra = __ldg(rank_text + slot0 + (uint64_t)qa * D + nr[ma] + (e & 0xffu));
+        const uint32_t rb = __ldg(rank_text + slot0 + (uint64_t)qb * D + nr[mb] + (e >> 8));
+        if (!(ra < rb)) {  // a is not before b: the pair is reversed (distinct suffixes are totally ordered)
+            sa[start] = (uint32_t)(b + pos0);
+            sa[start + 1] = (uint32_t)(a + pos0);
+        }
+    }
 }
 
 // Groups of 2..W elements, 32/W groups per warp.
@@ -175,14 +206,14 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
         for (uint32_t i = threadIdx.x; i < (uint32_t)C; i += THREADS) {
             const uint32_t p = i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS;
             s_pos[i] = p;
-            s_res[i] = p == INVALID_POS ? 0 : (uint8_t)(p % X);
+            s_res[i] = p == INVALID_POS ? 0 : (uint8_t)(p - fdiv(p, dcp->fx) * X);
             s_idx[i] = (uint16_t)i;
         }
         __syncthreads();
         for (uint32_t t = threadIdx.x; t < size * D; t += THREADS) {  // ranks, D consecutive words per element
             const uint32_t i = t / D, k = t - i * D;
             const uint32_t p = s_pos[i];
-            s_rk[t] = __ldg(rank_text + slot0 + (uint64_t)(p / X) * D + nr[s_res[i]] + k);
+            s_rk[t] = __ldg(rank_text + slot0 + (uint64_t)fdiv(p, dcp->fx) * D + nr[s_res[i]] + k);
         }
         __syncthreads();
         for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
