@@ -323,6 +323,21 @@ def run_gpu(args, world, rank, local):
         ms_e2e = float(t.item())
     e2e_value = world * n / GiB / (ms_e2e / e2e_steps / 1000.0)
 
+    lcp_line = None
+    if args.lcp:  # LCP of the built SA, device-resident (Phi + chunked Kasai)
+        d_lcp = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
+        ctx.build_lcp_device(d_text.data_ptr(), n, d_sa.data_ptr(), width, d_lcp.data_ptr(), 32)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            ctx.build_lcp_device(d_text.data_ptr(), n, d_sa.data_ptr(), width, d_lcp.data_ptr(), 32)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_lcp = e0.elapsed_time(e1) / 3
+        lcp_line = {"value": round(n / GiB / (ms_lcp / 1000.0), 4), "unit": "GiB/s", "ms": round(ms_lcp, 3),
+                    "call": "dcx_build_lcp, device pointers, uint32 LCP"}
+        del d_lcp
+
     # roofline of the dominant kernel (onesweep radix pass)
     s_last = stats[-1]
     bytes_radix = sum(s["bytes_radix"] for s in stats)
@@ -357,6 +372,8 @@ def run_gpu(args, world, rank, local):
             "build_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in s_last.items()},
             "clocks": clock,
         }
+        if lcp_line:
+            line["lcp"] = lcp_line
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             sample = min(n, args.cpu_sample_mib << 20)
@@ -757,6 +774,7 @@ def main():
     ap.add_argument("--cpu-sample-mib", type=int, default=256)
     ap.add_argument("--ref-sample-mib", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
     ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")

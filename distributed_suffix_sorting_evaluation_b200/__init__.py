@@ -41,6 +41,7 @@ DCX_DEVICE_PTRS = 1
 DCX_NO_PACKING = 2
 DCX_NO_REMAP = 4
 DCX_SERVE_BORROW = 8
+DCX_LCP_PERMUTED = 16
 
 SUPPORTED_DC = (3, 7, 13, 21, 31, 39, 57, 73, 91, 95, 133)
 
@@ -50,7 +51,7 @@ EXPORTED = (
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
-    "dcx_serve_submit_ex",
+    "dcx_serve_submit_ex", "dcx_build_lcp",
 )
 
 # serving request states (dcx_serve_poll)
@@ -128,6 +129,7 @@ def load_library(path: str | None = None):
     lib.dcx_dc_table.argtypes = [i32, vp, vp, vp, vp]
     lib.dcx_version.restype = ctypes.c_char_p
     lib.dcx_build_sa_noalloc.argtypes = [vp, u64, vp, vp]
+    lib.dcx_build_lcp.argtypes = [vp, vp, u64, vp, i32, vp, i32, u32]
     lib.dcx_check_sa.argtypes = [vp, vp, u64, vp, i32, u32, ctypes.POINTER(i32)]
     _lib = lib
     return lib
@@ -252,6 +254,24 @@ class Context:
                                      raw.ctypes.data if raw.size else None, sa_width, DCX_HOST_PTRS,
                                      ctypes.byref(ok)))
         return bool(ok.value)
+
+    def build_lcp(self, text, sa: np.ndarray, permuted: bool = False) -> np.ndarray:
+        """LCP array (or PLCP) of a host text and its SA (any integer array)."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        s = np.ascontiguousarray(np.asarray(sa).astype(np.uint64))
+        out = np.zeros(max(t.size, 1), np.uint64)
+        flags = DCX_HOST_PTRS | (DCX_LCP_PERMUTED if permuted else 0)
+        if t.size:
+            _check(self.lib.dcx_build_lcp(self.h, t.ctypes.data, t.size, s.ctypes.data, 64, out.ctypes.data, 64,
+                                          flags))
+        return out[: t.size]
+
+    def build_lcp_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int, lcp_ptr: int,
+                         lcp_width: int = 32, permuted: bool = False):
+        flags = DCX_DEVICE_PTRS | (DCX_LCP_PERMUTED if permuted else 0)
+        _check(self.lib.dcx_build_lcp(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
+                                      ctypes.c_void_p(lcp_ptr), lcp_width, flags))
 
     def check_sa_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int) -> bool:
         """GPU check of a device-resident SA against a device-resident text."""

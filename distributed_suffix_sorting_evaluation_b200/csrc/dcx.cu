@@ -36,6 +36,7 @@
 #include "radix.cuh"
 #include "segsort.cuh"
 #include "small_sa.cuh"
+#include "lcp.cuh"
 
 namespace dcx {
 
@@ -1448,6 +1449,48 @@ static bool check_one(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     return d2h_scalar(c, bad.get()) == 0;
 }
 
+// LCP (or PLCP with DCX_LCP_PERMUTED) of a text and its SA; lcp_width 32 or 64.
+static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, int sa_width, void* out,
+                      int lcp_width, uint32_t flags) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    if (!(sa_width == 32 || sa_width == 40 || sa_width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (!(lcp_width == 32 || lcp_width == 64)) throw Error(DCX_ERR_ARG, "lcp_width must be 32 or 64");
+    if (n == 0) return;
+    if (!text || !sa || !out) throw Error(DCX_ERR_ARG, "null pointer");
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    const size_t wb = sa_width / 8, lb = lcp_width / 8;
+    // padded text copy: the comparison loads read up to 15 bytes past the end
+    DBuf<uint8_t> t(&c, n + 16);
+    DCX_CUDA(cudaMemsetAsync(t.get() + n, 0, 16, c.stream));
+    DCX_CUDA(cudaMemcpyAsync(t.get(), text, n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+    DBuf<uint8_t> sa_in;
+    const void* dsa = sa;
+    if (!dev) {
+        sa_in = DBuf<uint8_t>(&c, n * wb);
+        DCX_CUDA(cudaMemcpyAsync(sa_in.get(), sa, n * wb, cudaMemcpyHostToDevice, c.stream));
+        dsa = sa_in.get();
+    }
+    DBuf<uint32_t> phi(&c, n), sa32(&c, n), plcp(&c, n);
+    k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(dsa, sa_width, n, phi.get(), sa32.get());
+    DCX_CHECK_LAUNCH();
+    sa_in.reset();
+    k_plcp<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(t.get(), n, phi.get(), plcp.get());
+    DCX_CHECK_LAUNCH();
+    phi.reset();
+    DBuf<uint8_t> stage;
+    void* dout = out;
+    if (!dev) {
+        stage = DBuf<uint8_t>(&c, n * lb);
+        dout = stage.get();
+    }
+    k_lcp_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), plcp.get(), n, dout, lcp_width,
+                                                        (flags & DCX_LCP_PERMUTED) != 0);
+    DCX_CHECK_LAUNCH();
+    c.launched(3);
+    if (!dev) DCX_CUDA(cudaMemcpyAsync(out, dout, n * lb, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 }  // namespace dcx
 
 #include "serve.cuh"
@@ -1626,6 +1669,16 @@ int dcx_build_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, voi
 
 int dcx_build_sa_strict(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags) {
     return build_entry(x, text, n, dc, w, out, flags, true);
+}
+
+int dcx_build_lcp(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, int sa_width, void* lcp_out,
+                  int lcp_width, uint32_t flags) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::build_lcp(x->c, text, n, sa, sa_width, lcp_out, lcp_width, flags);
+    });
 }
 
 int dcx_check_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, int sa_width, uint32_t flags,

@@ -113,6 +113,17 @@ int dcx_build_sa_strict(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, i
 int dcx_check_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
                  uint32_t flags, int* ok);
 
+/* ---- LCP ------------------------------------------------------------------- */
+/* Longest-common-prefix array of a text and its suffix array (sa_width 32, 40
+ * or 64 bits per entry): lcp_out[k] = lcp(SA[k], SA[k-1]), lcp_out[0] = 0, as
+ * libsais64_plcp + libsais64_lcp (libsais/include/libsais64.h:236-263) compute
+ * it; with DCX_LCP_PERMUTED the permuted array PLCP[i] = LCP[ISA[i]] instead.
+ * lcp_width is 32 or 64.  No counterpart in lightweight_dcx, whose SA is the
+ * usual input of this step.  Host or device pointers as for dcx_build_sa. */
+#define DCX_LCP_PERMUTED 16
+int dcx_build_lcp(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
+                  void* lcp_out, int lcp_width, uint32_t flags);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
  * caller can time builds with events recorded on it. */
 int dcx_get_stream(dcx_ctx* ctx, void** stream_out);

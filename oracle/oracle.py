@@ -99,6 +99,10 @@ def _load_sais():
         lib.libsais64.restype = ctypes.c_int64
         lib.libsais64_omp.argtypes = [_u8p, _i64p, ctypes.c_int64, ctypes.c_int64, _i64p, ctypes.c_int64]
         lib.libsais64_omp.restype = ctypes.c_int64
+        lib.libsais64_plcp.argtypes = [_u8p, _i64p, _i64p, ctypes.c_int64]
+        lib.libsais64_plcp.restype = ctypes.c_int64
+        lib.libsais64_lcp.argtypes = [_i64p, _i64p, _i64p, ctypes.c_int64]
+        lib.libsais64_lcp.restype = ctypes.c_int64
         _sais = lib
     return _sais
 
@@ -192,6 +196,24 @@ def libsais(text: np.ndarray, threads: int = 1) -> np.ndarray:
     if rc != 0:
         raise RuntimeError(f"libsais failed: {rc}")
     return sa
+
+
+def libsais_lcp(text: np.ndarray, sa: np.ndarray | None = None):
+    """(PLCP, LCP) of ``text`` by libsais64_plcp / libsais64_lcp (SA from libsais
+    unless given)."""
+    lib = _load_sais()
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    n = t.size
+    if n == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    s = libsais(t) if sa is None else np.ascontiguousarray(sa, dtype=np.int64)
+    plcp = np.zeros(n, np.int64)
+    lcp = np.zeros(n, np.int64)
+    if lib.libsais64_plcp(_ptr(t, _u8p), _ptr(s, _i64p), _ptr(plcp, _i64p), n) != 0:
+        raise RuntimeError("libsais64_plcp failed")
+    if lib.libsais64_lcp(_ptr(plcp, _i64p), _ptr(s, _i64p), _ptr(lcp, _i64p), n) != 0:
+        raise RuntimeError("libsais64_lcp failed")
+    return plcp, lcp
 
 
 def slow_sa(text: np.ndarray) -> np.ndarray:

@@ -105,3 +105,13 @@ def test_packing_choice(oracle):
     assert oracle.packing_for_sigma(3, 4) == (3, 1)
     assert oracle.packing_for_sigma(39, 20) == (5, 4)
     assert oracle.packing_for_sigma(39, 200) == (8, 5)
+
+
+def test_libsais_lcp_known_answer(oracle):
+    """mississippi: SA 10 7 4 1 0 9 8 6 3 5 2, LCP 0 1 1 4 0 0 1 0 2 1 3 (textbook values)."""
+    t = np.frombuffer(b"mississippi", np.uint8)
+    plcp, lcp = oracle.libsais_lcp(t)
+    assert list(oracle.libsais(t)) == [10, 7, 4, 1, 0, 9, 8, 6, 3, 5, 2]
+    assert list(lcp) == [0, 1, 1, 4, 0, 0, 1, 0, 2, 1, 3]
+    sa = oracle.libsais(t)
+    assert all(plcp[sa[k]] == lcp[k] for k in range(t.size))
