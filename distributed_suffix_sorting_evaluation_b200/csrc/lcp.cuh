@@ -12,7 +12,7 @@
 
 namespace dcx {
 
-constexpr uint32_t LCP_RUN = 1024;
+constexpr uint32_t LCP_RUN = 64;
 constexpr uint32_t PHI_NONE = 0xffffffffu;
 
 __device__ __forceinline__ uint64_t load_sa_u(const void* sa, uint64_t k, int width) {

@@ -192,11 +192,12 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
     uint16_t* tab = s_idx + C;                                      // [X * X]
     uint8_t* s_res = reinterpret_cast<uint8_t*>(tab + X * X);       // [C]
     load_dc_smem(*dcp, tab, nr);
+    constexpr uint8_t NO_ELEM = 0xff;  // residue of a padding slot (X <= 133 < 255)
     auto less = [&](uint32_t ia, uint32_t ib) -> bool {
-        const uint32_t pa = s_pos[ia], pb = s_pos[ib];
-        if (pa == INVALID_POS) return false;
-        if (pb == INVALID_POS) return true;
-        const uint16_t e = tab[s_res[ia] * X + s_res[ib]];
+        const uint32_t ra = s_res[ia], rb = s_res[ib];
+        if (ra == NO_ELEM) return false;
+        if (rb == NO_ELEM) return true;
+        const uint16_t e = tab[ra * X + rb];
         return s_rk[ia * D + (e & 0xffu)] < s_rk[ib * D + (e >> 8)];
     };
     for (uint64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
@@ -206,7 +207,7 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
         for (uint32_t i = threadIdx.x; i < (uint32_t)C; i += THREADS) {
             const uint32_t p = i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS;
             s_pos[i] = p;
-            s_res[i] = p == INVALID_POS ? 0 : (uint8_t)(p - fdiv(p, dcp->fx) * X);
+            s_res[i] = p == INVALID_POS ? NO_ELEM : (uint8_t)(p - fdiv(p, dcp->fx) * X);
             s_idx[i] = (uint16_t)i;
         }
         __syncthreads();
@@ -216,10 +217,13 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
             s_rk[t] = __ldg(rank_text + slot0 + (uint64_t)fdiv(p, dcp->fx) * D + nr[s_res[i]] + k);
         }
         __syncthreads();
+#pragma unroll
         for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
+#pragma unroll
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
                 for (uint32_t p = threadIdx.x; p < (uint32_t)C / 2; p += THREADS) {
-                    const uint32_t i = 2 * j * (p / j) + (p % j);
+                    const uint32_t i = ((p & ~(j - 1)) << 1) | (p & (j - 1));  // j is a power of two
                     const uint32_t q = i + j;
                     const bool up = (i & k) == 0;
                     const uint32_t a = s_idx[i], b = s_idx[q];
