@@ -486,6 +486,108 @@ static DBuf<T> upload(Ctx& c, const std::vector<T>& v) {
     return d;
 }
 
+// Tie groups: maximal runs of the sorted order whose elements after the first
+// have head 0, binned by size class (tie_class) into gstart/gsize.
+struct TieGroups {
+    uint64_t G = 0;
+    std::vector<uint32_t> counts;  // groups per class
+    std::vector<uint64_t> off;     // first group of each class in gstart/gsize
+    DBuf<uint32_t> gstart, gsize;
+};
+
+static TieGroups group_ties(Ctx& c, const uint8_t* head, uint64_t N) {
+    TieGroups tg;
+    DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1);
+    OpGroups op{head, N, starts.get(), ends.get()};
+    const uint64_t tot = device_scan<uint64_t>(c, op, N);
+    c.alg(N);
+    tg.G = tot & 0xffffffffull;
+    tg.counts.assign(TIE_CLASSES, 0);
+    tg.off.assign(TIE_CLASSES + 1, 0);
+    if (tg.G == 0) return tg;
+    DBuf<uint32_t> cnt(&c, 2 * TIE_CLASSES);
+    DCX_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * TIE_CLASSES * 4, c.stream));
+    k_tie_classify<<<grid_for(tg.G, 256), 256, 0, c.stream>>>(tg.G, starts.get(), ends.get(), cnt.get());
+    DCX_CHECK_LAUNCH();
+    DCX_CUDA(cudaMemcpyAsync(tg.counts.data(), cnt.get(), TIE_CLASSES * 4, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<uint32_t> cursor(TIE_CLASSES, 0);
+    for (int k = 0; k < TIE_CLASSES; k++) {
+        cursor[k] = (uint32_t)tg.off[k];
+        tg.off[k + 1] = tg.off[k] + tg.counts[k];
+    }
+    DCX_CUDA(cudaMemcpyAsync(cnt.get() + TIE_CLASSES, cursor.data(), TIE_CLASSES * 4, cudaMemcpyHostToDevice, c.stream));
+    tg.gstart = DBuf<uint32_t>(&c, tg.G);
+    tg.gsize = DBuf<uint32_t>(&c, tg.G);
+    k_tie_bin<<<grid_for(tg.G, 256), 256, 0, c.stream>>>(tg.G, starts.get(), ends.get(), cnt.get() + TIE_CLASSES,
+                                                          tg.gstart.get(), tg.gsize.get());
+    DCX_CHECK_LAUNCH();
+    c.launched(4);
+    return tg;
+}
+
+static RefinePlan8 make_refine8(uint64_t B, uint32_t P) {
+    RefinePlan8 r8{};
+    r8.P = P;
+    r8.m = (P + 7) / 8;
+    r8.r = P - 8 * (r8.m - 1);
+    r8.B = B;
+    r8.B2 = B * B;
+    r8.B4 = r8.B2 * r8.B2;
+    r8.pow8 = r8.B4 * r8.B4;  // only used when m > 1, i.e. B^8 < 2^64
+    r8.powr = 1;
+    for (uint32_t i = 0; i < r8.r; i++) r8.powr *= B;
+    return r8;
+}
+
+template <int C, int T, int W>
+static void launch_refine_seg(Ctx& c, const uint8_t* text, SegView sv, const uint32_t* segw, const uint32_t* gstart,
+                              const uint32_t* gsize, uint64_t ng, uint32_t* sa, uint8_t* head,
+                              const RefineSegPlan& plan) {
+    const size_t shm = refine_seg_smem<C, W>();
+    DCX_CUDA(cudaFuncSetAttribute(k_refine_seg<C, T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    int per_sm = 0;
+    DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_seg<C, T, W>, T, shm));
+    const uint64_t grid = std::min<uint64_t>(ng, 148ull * std::max(per_sm, 1));
+    k_refine_seg<C, T, W><<<(unsigned)grid, T, shm, c.stream>>>(text, sv, segw, gstart, gsize, ng, sa, head, plan);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+}
+
+// Groups of two (class 0) and of 3..32 (classes 1-4).
+template <int W>
+static void refine_small_w(Ctx& c, const uint8_t* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
+                           uint32_t* sa, uint8_t* head, const RefineSegPlan& plan) {
+    if (tg.counts[0]) {
+        k_refine_pair<W><<<grid_for(tg.counts[0], 256, 148 * 16), 256, 0, c.stream>>>(
+            text, sv, segw, tg.gstart.get(), tg.counts[0], sa, head, plan);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    }
+    const uint64_t g0 = tg.off[1], ng = tg.off[5] - g0;
+    if (ng) {
+        k_refine_warp<W><<<grid_for(ng * 32, 256, 148 * 16), 256, 0, c.stream>>>(
+            text, sv, segw, tg.gstart.get() + g0, tg.gsize.get() + g0, ng, sa, head, plan);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    }
+}
+
+template <int C, int T>
+static void refine_seg_class(Ctx& c, const uint8_t* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
+                             int cls_lo, int cls_hi, uint32_t* sa, uint8_t* head, const RefineSegPlan& plan) {
+    const uint64_t g0 = tg.off[cls_lo], ng = tg.off[cls_hi + 1] - g0;
+    if (!ng) return;
+    const uint32_t* gs = tg.gstart.get() + g0;
+    const uint32_t* gz = tg.gsize.get() + g0;
+    switch (plan.W) {
+        case 1: launch_refine_seg<C, T, 1>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+        case 2: launch_refine_seg<C, T, 2>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+        case 3: launch_refine_seg<C, T, 3>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+        default: launch_refine_seg<C, T, 4>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Phase 1: sort all N suffixes of the level by (text, first L chars).
 // Produces the sorted positions `sa`, head flags (1 where the key differs from
@@ -588,12 +690,56 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         }
     }
 
-    // refinement rounds for tied windows (a group never spans two texts)
+    // refinement of tied windows (a group never spans two texts)
     uint32_t covered = P0;
+    uint8_t* hd = head.get();  // head flags the global rounds work on
+    TieGroups tg;
+    DBuf<uint8_t> head2;
+    if (covered < L && sizeof(CharT) == 1 && B <= 256 && ((uintptr_t)text & 7) == 0) {
+        // Groups of up to 2048 elements are sorted by the whole rest of the window
+        // inside one CTA each; only larger groups take the global radix rounds.
+        const uint32_t rem = L - covered;
+        const uint32_t cpw = std::min<uint32_t>(64, max_chars_in_bits(B, 64));
+        const uint32_t W = (rem + cpw - 1) / cpw;
+        if (W <= (uint32_t)RSEG_MAX_W) {
+            tg = group_ties(c, hd, N);
+            RefineSegPlan plan{};
+            plan.W = W;
+            for (uint32_t w = 0; w < W; w++) {
+                plan.off[w] = covered + w * cpw;
+                plan.rp[w] = make_refine8(B, std::min(cpw, rem - w * cpw));
+            }
+            const uint8_t* t8 = reinterpret_cast<const uint8_t*>(text);
+            const uint32_t* sw = SEGK ? segw.get() : nullptr;
+            switch (W) {
+                case 1: refine_small_w<1>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+                case 2: refine_small_w<2>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+                case 3: refine_small_w<3>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+                default: refine_small_w<4>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+            }
+            refine_seg_class<64, 32>(c, t8, sv, sw, tg, 5, 5, sa.get(), hd, plan);
+            refine_seg_class<256, 128>(c, t8, sv, sw, tg, 6, 7, sa.get(), hd, plan);
+            refine_seg_class<1024, 512>(c, t8, sv, sw, tg, 8, 9, sa.get(), hd, plan);
+            refine_seg_class<2048, 512>(c, t8, sv, sw, tg, 10, 10, sa.get(), hd, plan);
+            const uint64_t small = tg.off[TIE_CLASSES - 1];  // groups of at most 2048
+            if (tg.counts[TIE_CLASSES - 1]) {
+                // the global rounds see the small groups as resolved
+                head2 = DBuf<uint8_t>(&c, N);
+                DCX_CUDA(cudaMemcpyAsync(head2.get(), hd, N, cudaMemcpyDeviceToDevice, c.stream));
+                k_group_flags<<<grid_for(small * 32, 256), 256, 0, c.stream>>>(tg.gstart.get(), tg.gsize.get(), small,
+                                                                              head2.get(), nullptr);
+                DCX_CHECK_LAUNCH();
+                c.launched();
+                hd = head2.get();
+            } else {
+                covered = L;
+            }
+        }
+    }
     while (covered < L) {
         DBuf<uint32_t> slot(&c, N), grp(&c, N), tpos(&c, N), tseg;
         if (SEGK) tseg = DBuf<uint32_t>(&c, N);
-        OpTied op{head.get(), N, sa.get(), SEGK ? segw.get() : nullptr, slot.get(), grp.get(), tpos.get(),
+        OpTied op{hd, N, sa.get(), SEGK ? segw.get() : nullptr, slot.get(), grp.get(), tpos.get(),
                   SEGK ? tseg.get() : nullptr};
         const uint64_t tot = device_scan<uint64_t>(c, op, N);
         c.alg(N + N / 2);
@@ -621,16 +767,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         const bool swar = sizeof(CharT) == 1 && B <= 256 && Pr <= 64 && ((uintptr_t)text & 7) == 0;
         if (swar) {
             // byte text: aligned word loads + SWAR digit folding
-            RefinePlan8 r8{};
-            r8.P = Pr;
-            r8.m = (Pr + 7) / 8;
-            r8.r = Pr - 8 * (r8.m - 1);
-            r8.B = B;
-            r8.B2 = B * B;
-            r8.B4 = r8.B2 * r8.B2;
-            r8.pow8 = r8.B4 * r8.B4;  // only used when m > 1, i.e. B^8 < 2^64
-            r8.powr = 1;
-            for (uint32_t i = 0; i < r8.r; i++) r8.powr *= B;
+            const RefinePlan8 r8 = make_refine8(B, Pr);
             const uint8_t* t8 = reinterpret_cast<const uint8_t*>(text);
             DCX_CUDA(cudaFuncSetAttribute(k_keys_refine8<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
             DCX_CUDA(cudaFuncSetAttribute(k_keys_refine8<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 << 10));
@@ -656,12 +793,18 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         int f = radix_sort(c, kwr, cnt, s);
         KeyWords kk{};
         for (uint32_t w = 0; w < kwr; w++) kk.w[w] = s.k[f][w];
-        k_refine_scatter<<<grid_for(cnt, 256), 256, 0, c.stream>>>(cnt, slot.get(), kk, kwr, s.v[f], sa.get(),
-                                                                   head.get());
+        k_refine_scatter<<<grid_for(cnt, 256), 256, 0, c.stream>>>(cnt, slot.get(), kk, kwr, s.v[f], sa.get(), hd);
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(cnt * (4 + kwr * 4 * 2 + 4 + 4 + 1));
         covered += Pr;
+    }
+    if (hd != head.get()) {  // big groups' flags back into the real head array
+        const uint64_t g0 = tg.off[TIE_CLASSES - 1], nbig = tg.counts[TIE_CLASSES - 1];
+        k_group_flags<<<grid_for(nbig * 32, 256), 256, 0, c.stream>>>(tg.gstart.get() + g0, tg.gsize.get() + g0, nbig,
+                                                                     head.get(), hd);
+        DCX_CHECK_LAUNCH();
+        c.launched();
     }
 }
 
@@ -756,33 +899,12 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
 
 static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, const uint32_t* rank_text,
                       const DcHost& dc, TieSeg ts) {
-    DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1);
-    OpGroups op{head, N, starts.get(), ends.get()};
-    const uint64_t tot = device_scan<uint64_t>(c, op, N);
-    c.alg(N);
-    const uint64_t G = tot & 0xffffffffull;
+    TieGroups tg = group_ties(c, head, N);
+    const uint64_t G = tg.G;
     if (G == 0) return;
-    DBuf<uint32_t> cnt(&c, 2 * TIE_CLASSES);
-    DCX_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * TIE_CLASSES * 4, c.stream));
-    k_tie_classify<<<grid_for(G, 256), 256, 0, c.stream>>>(G, starts.get(), ends.get(), cnt.get());
-    DCX_CHECK_LAUNCH();
-    std::vector<uint32_t> counts(TIE_CLASSES);
-    DCX_CUDA(cudaMemcpyAsync(counts.data(), cnt.get(), TIE_CLASSES * 4, cudaMemcpyDeviceToHost, c.stream));
-    DCX_CUDA(cudaStreamSynchronize(c.stream));
-    std::vector<uint32_t> cursor(TIE_CLASSES, 0);
-    uint64_t acc = 0;
-    for (int k = 0; k < TIE_CLASSES; k++) {
-        cursor[k] = (uint32_t)acc;
-        acc += counts[k];
-    }
-    DCX_CUDA(cudaMemcpyAsync(cnt.get() + TIE_CLASSES, cursor.data(), TIE_CLASSES * 4, cudaMemcpyHostToDevice, c.stream));
-    DBuf<uint32_t> gstart(&c, G), gsize(&c, G);
-    k_tie_bin<<<grid_for(G, 256), 256, 0, c.stream>>>(G, starts.get(), ends.get(), cnt.get() + TIE_CLASSES,
-                                                       gstart.get(), gsize.get());
-    DCX_CHECK_LAUNCH();
-    c.launched(2);
-    starts.reset();
-    ends.reset();
+    const std::vector<uint32_t>& counts = tg.counts;
+    DBuf<uint32_t>& gstart = tg.gstart;
+    DBuf<uint32_t>& gsize = tg.gsize;
     const DcDev* dcd = c.dc_dev[dc.X];
     switch (dc.D) {
 #define DCX_TIE(DV) \

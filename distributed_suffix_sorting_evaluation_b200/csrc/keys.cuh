@@ -299,6 +299,30 @@ __device__ __forceinline__ uint64_t swar_digits8(uint64_t w, const RefinePlan8& 
     return (t32 & 0xffffffffull) * rp.B4 + (t32 >> 32);
 }
 
+// Base-B value of the rp.P chars at s (chars at or past `end` count as 0).
+__device__ __forceinline__ uint64_t window_value8(const uint64_t* __restrict__ tw0, uint64_t s, uint64_t end,
+                                                  const RefinePlan8& rp) {
+    const uint64_t a0 = s & ~7ull;
+    const uint32_t shb = (uint32_t)(s - a0) * 8u;
+    uint64_t w[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++)  // words at or past the end hold only zero chars: not read
+        w[k] = ((uint32_t)k <= rp.m && a0 + 8ull * k < end) ? __ldg(tw0 + (a0 >> 3) + k) : 0ull;
+    const uint64_t v = end > s ? end - s : 0;  // window chars inside the text
+    uint64_t key = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if ((uint32_t)k >= rp.m) break;
+        uint64_t cw = shb ? (w[k] >> shb) | (w[k + 1] << (64u - shb)) : w[k];
+        const int64_t vk = (int64_t)v - 8 * k;
+        if (vk < 8) cw = vk <= 0 ? 0ull : cw & ((1ull << (8 * vk)) - 1ull);
+        const bool last = (uint32_t)k == rp.m - 1;
+        if (last && rp.r < 8) cw <<= 8u * (8u - rp.r);  // drop chars past the window; keep r low digits
+        key = key * (last ? rp.powr : rp.pow8) + swar_digits8(cw, rp);
+    }
+    return key;
+}
+
 template <int KW>
 __global__ __launch_bounds__(256) void k_keys_refine8(const uint8_t* __restrict__ text, SegView sv, uint64_t count,
                                                       const uint32_t* __restrict__ tpos,
@@ -312,25 +336,7 @@ __global__ __launch_bounds__(256) void k_keys_refine8(const uint8_t* __restrict_
          j += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t pos = tpos[j];
         const uint64_t end = seg_end(sv, tseg ? tseg[j] : 0u);
-        const uint64_t s = (uint64_t)pos + off;
-        const uint64_t a0 = s & ~7ull;
-        const uint32_t shb = (uint32_t)(s - a0) * 8u;
-        uint64_t w[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++)  // words at or past the end hold only zero chars: not read
-            w[k] = ((uint32_t)k <= rp.m && a0 + 8ull * k < end) ? __ldg(tw0 + (a0 >> 3) + k) : 0ull;
-        const uint64_t v = end > s ? end - s : 0;  // window chars inside the text
-        uint64_t key = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            if ((uint32_t)k >= rp.m) break;
-            uint64_t cw = shb ? (w[k] >> shb) | (w[k + 1] << (64u - shb)) : w[k];
-            const int64_t vk = (int64_t)v - 8 * k;
-            if (vk < 8) cw = vk <= 0 ? 0ull : cw & ((1ull << (8 * vk)) - 1ull);
-            const bool last = (uint32_t)k == rp.m - 1;
-            if (last && rp.r < 8) cw <<= 8u * (8u - rp.r);  // drop chars past the window; keep r low digits
-            key = key * (last ? rp.powr : rp.pow8) + swar_digits8(cw, rp);
-        }
+        const uint64_t key = window_value8(tw0, (uint64_t)pos + off, end, rp);
         uint32_t kk[KW + 1];
         kk[0] = (uint32_t)key;
         if (KW > 1) kk[1] = (uint32_t)(key >> 32);
@@ -341,6 +347,190 @@ __global__ __launch_bounds__(256) void k_keys_refine8(const uint8_t* __restrict_
         hist_add<KW + 1>(sh, kk);
     }
     hist_flush(sh, 4 * (KW + 1) * RADIX, hist);
+}
+
+// Refinement of small tie groups inside one CTA: the elements of a group (up
+// to C, all of one text) get the rest of their window, chars [off, L), as W
+// words of base-B chunks (lexicographic order of the words = order of the
+// chars), a bitonic network in shared memory sorts 16-bit indices by them, and
+// the group is written back with head flags where the words change.  Equal
+// windows stay tied (head 0) for the cover-rank tie break.  The CTA loops over
+// groups.
+constexpr int RSEG_MAX_W = 4;
+struct RefineSegPlan {
+    uint32_t W;                       // words per element
+    uint32_t off[RSEG_MAX_W];         // first char of each word, relative to the position
+    RefinePlan8 rp[RSEG_MAX_W];
+};
+
+template <int C, int THREADS, int W>
+__global__ __launch_bounds__(THREADS) void k_refine_seg(const uint8_t* __restrict__ text, SegView sv,
+                                                        const uint32_t* __restrict__ segw,
+                                                        const uint32_t* __restrict__ gstart,
+                                                        const uint32_t* __restrict__ gsize, uint64_t ngroups,
+                                                        uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
+                                                        RefineSegPlan plan) {
+    static_assert(C <= 65536 && (C & (C - 1)) == 0, "power-of-two groups, 16-bit indices");
+    extern __shared__ __align__(16) uint64_t s_dyn64[];  // refine_seg_smem<C, W>() bytes
+    uint64_t(*s_key)[C] = reinterpret_cast<uint64_t(*)[C]>(s_dyn64);             // [W][C]
+    uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_dyn64 + (size_t)W * C);      // [C]
+    uint16_t* s_idx = reinterpret_cast<uint16_t*>(s_pos + C);                    // [C]
+    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
+    for (uint64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const uint32_t start = gstart[g], size = gsize[g];
+        const uint64_t end = seg_end(sv, segw ? segw[start] : 0u);
+        for (uint32_t i = threadIdx.x; i < (uint32_t)C; i += THREADS) {
+            s_idx[i] = (uint16_t)i;
+            if (i < size) {
+                const uint32_t p = sa[start + i];
+                s_pos[i] = p;
+#pragma unroll
+                for (int w = 0; w < W; w++) s_key[w][i] = window_value8(tw0, (uint64_t)p + plan.off[w], end, plan.rp[w]);
+            }
+        }
+        __syncthreads();
+        auto less = [&](uint32_t a, uint32_t b) -> bool {  // padding (index >= size) sorts last
+            if (a >= size) return false;
+            if (b >= size) return true;
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                const uint64_t ka = s_key[w][a], kb = s_key[w][b];
+                if (ka != kb) return ka < kb;
+            }
+            return false;
+        };
+#pragma unroll
+        for (uint32_t k = 2; k <= (uint32_t)C; k <<= 1) {
+#pragma unroll
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+                for (uint32_t p = threadIdx.x; p < (uint32_t)C / 2; p += THREADS) {
+                    const uint32_t i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
+                    const uint32_t q = i + j;
+                    const uint32_t a = s_idx[i], b = s_idx[q];
+                    if ((i & k) == 0 ? less(b, a) : less(a, b)) {
+                        s_idx[i] = (uint16_t)b;
+                        s_idx[q] = (uint16_t)a;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t i = threadIdx.x; i < size; i += THREADS) {
+            const uint32_t a = s_idx[i];
+            sa[start + i] = s_pos[a];
+            if (i > 0) {  // the group's first element keeps its head flag
+                const uint32_t b = s_idx[i - 1];
+                bool diff = false;
+#pragma unroll
+                for (int w = 0; w < W; w++) diff |= s_key[w][a] != s_key[w][b];
+                head[start + i] = diff ? 1 : 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Groups of exactly two: one thread per group.
+template <int W>
+__global__ __launch_bounds__(256) void k_refine_pair(const uint8_t* __restrict__ text, SegView sv,
+                                                     const uint32_t* __restrict__ segw,
+                                                     const uint32_t* __restrict__ gstart, uint64_t ngroups,
+                                                     uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
+                                                     RefineSegPlan plan) {
+    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t start = gstart[g];
+        const uint64_t end = seg_end(sv, segw ? segw[start] : 0u);
+        const uint32_t a = sa[start], b = sa[start + 1];
+        int cmp = 0;  // sign of key(a) - key(b)
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            if (cmp) break;
+            const uint64_t ka = window_value8(tw0, (uint64_t)a + plan.off[w], end, plan.rp[w]);
+            const uint64_t kb = window_value8(tw0, (uint64_t)b + plan.off[w], end, plan.rp[w]);
+            cmp = ka < kb ? -1 : (ka > kb ? 1 : 0);
+        }
+        if (cmp > 0) {
+            sa[start] = b;
+            sa[start + 1] = a;
+        }
+        head[start + 1] = cmp != 0;
+    }
+}
+
+// Groups of 3..32 elements: one warp per group, one element per lane, a
+// bitonic network over the lanes with shuffles.
+template <int W>
+__global__ __launch_bounds__(256) void k_refine_warp(const uint8_t* __restrict__ text, SegView sv,
+                                                     const uint32_t* __restrict__ segw,
+                                                     const uint32_t* __restrict__ gstart,
+                                                     const uint32_t* __restrict__ gsize, uint64_t ngroups,
+                                                     uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
+                                                     RefineSegPlan plan) {
+    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += warps) {
+        const uint32_t start = gstart[g], size = gsize[g];
+        const uint64_t end = seg_end(sv, segw ? segw[start] : 0u);
+        bool valid = lane < size;
+        uint32_t p = valid ? sa[start + lane] : 0u;
+        uint64_t key[W];
+#pragma unroll
+        for (int w = 0; w < W; w++) key[w] = valid ? window_value8(tw0, (uint64_t)p + plan.off[w], end, plan.rp[w]) : 0ull;
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const bool ov = __shfl_xor_sync(0xffffffffu, valid, j);
+                const uint32_t op = __shfl_xor_sync(0xffffffffu, p, j);
+                uint64_t ok[W];
+#pragma unroll
+                for (int w = 0; w < W; w++) ok[w] = __shfl_xor_sync(0xffffffffu, key[w], j);
+                // other < me / me < other (invalid lanes sort last)
+                int c = 0;
+#pragma unroll
+                for (int w = 0; w < W; w++)
+                    if (!c && ok[w] != key[w]) c = ok[w] < key[w] ? -1 : 1;
+                const bool o_less = ov && (!valid || c < 0);
+                const bool m_less = valid && (!ov || c > 0);
+                const bool up = (k == 32) || ((lane & k) == 0);
+                const bool lower = (lane & j) == 0;
+                if ((lower == up) ? o_less : m_less) {
+                    valid = ov;
+                    p = op;
+#pragma unroll
+                    for (int w = 0; w < W; w++) key[w] = ok[w];
+                }
+            }
+        }
+        bool diff = false;
+#pragma unroll
+        for (int w = 0; w < W; w++) diff |= __shfl_up_sync(0xffffffffu, key[w], 1) != key[w];
+        if (valid) {
+            sa[start + lane] = p;
+            if (lane > 0) head[start + lane] = diff;
+        }
+    }
+}
+
+template <int C, int W>
+constexpr size_t refine_seg_smem() {
+    return sizeof(uint64_t) * W * C + sizeof(uint32_t) * C + sizeof(uint16_t) * C;
+}
+
+// Sets (value 1) or copies (from src) the flags of the elements of groups.
+__global__ void k_group_flags(const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize, uint64_t ngroups,
+                              uint8_t* __restrict__ dst, const uint8_t* __restrict__ src) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t g = warp; g < ngroups; g += warps) {
+        const uint32_t st = gstart[g], sz = gsize[g];
+        for (uint32_t i = lane; i < sz; i += 32) dst[st + i] = src ? src[st + i] : (uint8_t)1;
+    }
 }
 
 }  // namespace dcx
