@@ -265,6 +265,8 @@ def run_gpu(args, world, rank, local):
     d_sa = torch.empty(n * wb, dtype=torch.uint8, device=f"cuda:{local}")
     host_sa = torch.empty(n * wb, dtype=torch.uint8, pin_memory=True)
     ctx = Context(local)
+    if args.recursion_dc:
+        ctx.set_option("recursion_dc", args.recursion_dc)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     torch.cuda.synchronize()
 
@@ -775,6 +777,7 @@ def main():
     ap.add_argument("--ref-sample-mib", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
+    ap.add_argument("--recursion-dc", type=int, default=0, help="difference cover of the recursion levels")
     ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")
