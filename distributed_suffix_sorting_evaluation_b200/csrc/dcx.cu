@@ -605,10 +605,12 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     uint32_t P0 = std::min<uint32_t>(L, max_chars_in_bits_k(B, 32 * std::min(words_full, kw0_max), K));
     if (depth == 0 && c.level0_entropy > 0.05) {
         // Shortest byte-aligned prefix whose expected random collisions stay near
-        // 1% of N: P * H >= log2(N) + 6, with H the order-0 entropy discounted by
+        // 1% of the longest text n: P * H >= log2(n) + 6, with H the order-0 entropy discounted by
         // 5% for context dependence.  Ties left over are resolved exactly by the
         // refinement rounds, so this only trades passes against refinement work.
-        const double need = std::log2((double)N) + 6.0;
+        uint64_t longest = 1;  // windows of different texts never collide (text id digit)
+        for (uint32_t t = 0; t < K; t++) longest = std::max<uint64_t>(longest, sg.len(t) + 1);
+        const double need = std::log2((double)longest) + 6.0;
         uint32_t P = (uint32_t)std::ceil(need / (0.95 * c.level0_entropy));
         P = std::max<uint32_t>(1, std::min(P, P0));
         const uint32_t bytes = (key_bits_k(B, P, K) + 7) / 8;
@@ -623,6 +625,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     const uint32_t kwt = kw;
 
     // round 0
+    unsigned long long round0_ties = 0;
     {
         DBuf<uint32_t> keys[2][3];
         DBuf<uint32_t> vals[2];
@@ -675,10 +678,12 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         KeyWords kk{};
         for (uint32_t w = 0; w < kwt; w++) kk.w[w] = s.k[f][w];
         head = DBuf<uint8_t>(&c, N);
-        k_heads<<<grid_for(N, 256), 256, 0, c.stream>>>(kk, kwt, N, head.get());
+        DCX_CUDA(cudaMemsetAsync(c.d_h256, 0, 8, c.stream));
+        k_heads<<<grid_for(N, 256), 256, 0, c.stream>>>(kk, kwt, N, head.get(), c.d_h256);
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(N * kwt * 4 + N);
+        round0_ties = d2h_scalar(c, c.d_h256);
         sa = std::move(vals[f]);
         if (SEGK) {
             // the sort is text-major, so text s owns sorted slots [start[s], start[s+1])
@@ -691,7 +696,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     }
 
     // refinement of tied windows (a group never spans two texts)
-    uint32_t covered = P0;
+    uint32_t covered = round0_ties ? P0 : L;  // nothing tied: every window is already distinct
     uint8_t* hd = head.get();  // head flags the global rounds work on
     TieGroups tg;
     DBuf<uint8_t> head2;
@@ -1029,7 +1034,8 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
     const uint32_t* segw_p = K > 1 ? segw.get() : nullptr;
 
     // ---- phase 2: names
-    DBuf<uint32_t> s_pos(&c, m), s_seg(&c, m), s_grp(&c, m);
+    DBuf<uint32_t> s_pos(&c, m), s_seg, s_grp(&c, m);
+    if (K > 1) s_seg = DBuf<uint32_t>(&c, m);  // one text: every sample's text is 0
     {
         OpSamples op{head.get(), sa.get(), segw_p, dfl.get(), ls, s_pos.get(), s_seg.get(), s_grp.get(), m};
         const uint64_t tot = device_scan<uint64_t>(c, op, N);

@@ -156,7 +156,11 @@ struct KeyWords {
     const uint32_t* w[12];
 };
 
-__global__ void k_heads(KeyWords k, uint32_t kw, uint64_t N, uint8_t* __restrict__ head) {
+// Head flags of a sorted key array; *ties (zeroed by the caller) receives the
+// number of elements equal to their predecessor.
+__global__ void k_heads(KeyWords k, uint32_t kw, uint64_t N, uint8_t* __restrict__ head,
+                        unsigned long long* __restrict__ ties) {
+    uint32_t t = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
         uint8_t h = 1;
         if (i > 0) {
@@ -164,7 +168,10 @@ __global__ void k_heads(KeyWords k, uint32_t kw, uint64_t N, uint8_t* __restrict
             for (uint32_t w = 0; w < kw; w++) h |= k.w[w][i] != k.w[w][i - 1];
         }
         head[i] = h;
+        t += !h;
     }
+    t = __reduce_add_sync(0xffffffffu, t);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(ties, (unsigned long long)t);
 }
 
 // ---- scan operators (two 32-bit counters packed in a uint64) ------------------
@@ -279,7 +286,7 @@ struct OpSamples {
             if (j >= cap) return;
             const uint32_t sg = segw ? segw[k] : 0u;
             s_pos[j] = (uint32_t)(sa[k] - ls.start[sg]);
-            s_seg[j] = sg;
+            if (s_seg) s_seg[j] = sg;
             s_grp[j] = (uint32_t)ex + (uint32_t)v;
         }
     }
@@ -315,7 +322,7 @@ __global__ void k_scatter_samples(uint64_t m, const uint32_t* __restrict__ s_pos
                                   const DcFlags* __restrict__ f, LevelSeg ls, uint64_t* __restrict__ srec) {
     const DcFlags& F = *f;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = ls.rbase[s_seg[j]] + slot_of_local(s_pos[j], F);
+        const uint64_t k = ls.rbase[s_seg ? s_seg[j] : 0u] + slot_of_local(s_pos[j], F);
         srec[k] = (uint64_t)name[j] | ((uint64_t)uniq[j] << 32) | ((uint64_t)j << 33);
     }
 }
