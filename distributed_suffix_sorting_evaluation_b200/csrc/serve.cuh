@@ -384,6 +384,9 @@ private:
                     continue;
                 }
                 if (!b.reqs.empty() && (text_bytes + r->n > cap || b.reqs.size() >= batch_texts_)) break;
+                // a long text is built alone: one text per sort amortises nothing, and the
+                // single-text pipeline is the faster one for it
+                if (!b.reqs.empty() && (r->n >= solo_bytes_ || b.reqs[0]->n >= solo_bytes_)) break;
                 if (reserved_ + r->footprint > budget_) break;  // first come, first served
                 reserved_ += r->footprint;
                 b.scratch += r->footprint - serve_result_bytes(r->n, width);
@@ -569,6 +572,7 @@ private:
     uint64_t budget_, batch_bytes_;
     uint32_t batch_texts_;
     uint64_t express_bytes_, express_batch_bytes_;
+    uint64_t solo_bytes_ = 32ull << 20;  // texts at least this long form a batch of their own
     PinnedArena arena_;
     std::mutex mu_, copy_mu_;
     std::condition_variable cv_work_, cv_done_;

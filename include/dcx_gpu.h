@@ -184,7 +184,8 @@ typedef struct dcx_serve_stats {
  * "serve_express_bytes" (default 4 MiB): lane 0 serves the requests longer
  * than this (all requests when it is the only lane), uploading its next batch
  * while it builds the current one; the other lanes, on high-priority streams,
- * serve the shorter ones in batches of at most 4x it.  Each class is served in
+ * serve the shorter ones in batches of at most 4x it.  A text of 32 MiB or more
+ * is always built in a batch of its own.  Each class is served in
  * arrival order, long builds run one at a time and short requests do not wait
  * behind them. */
 int dcx_serve_submit(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width,
