@@ -267,6 +267,9 @@ def run_gpu(args, world, rank, local):
     ctx = Context(local)
     if args.recursion_dc:
         ctx.set_option("recursion_dc", args.recursion_dc)
+    for kv in args.option:
+        k, v = kv.split("=", 1)
+        ctx.set_option(k, float(v))
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     torch.cuda.synchronize()
 
@@ -783,6 +786,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
     ap.add_argument("--recursion-dc", type=int, default=0, help="difference cover of the recursion levels")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="context option (dcx_set_option) for the single-text workloads")
     ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")

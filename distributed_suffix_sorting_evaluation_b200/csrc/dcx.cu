@@ -221,6 +221,7 @@ struct DBuf {
     size_t n = 0;
     DBuf() = default;
     DBuf(Ctx* ctx, size_t count);
+    DBuf(Ctx* ctx, size_t count, bool io);  // io: the context's staging pool (see Ctx::io_pool)
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
     DBuf(DBuf&& o) noexcept { *this = std::move(o); }
@@ -248,6 +249,11 @@ struct Ctx {
     uint32_t epoch = 0;
     uint32_t* h_pinned = nullptr;   // pinned staging for small transfers (PINNED_WORDS words)
     cudaMemPool_t pool = nullptr;   // own memory pool (serving lanes); null = the device's default pool
+    // Staging buffers of host-pointer calls (text copy, SA before its download)
+    // live in a pool of their own: placed among the build's scratch they would
+    // split the scratch pool's free blocks differently from one call type to the
+    // next and force the pool to map new memory inside the build.
+    cudaMemPool_t io_pool = nullptr;
     std::map<uint32_t, DcHost> dc_host;
     std::map<uint32_t, DcFlags*> dc_flags_dev;  // per X (samples_before filled per level on a copy)
     std::map<uint32_t, DcDev*> dc_dev;
@@ -257,13 +263,14 @@ struct Ctx {
     std::vector<uint8_t> trace_uniq;
     std::mutex build_mu;
 
-    void* alloc(size_t bytes) {
+    void* alloc(size_t bytes, bool io = false) {
         if (bytes == 0) bytes = 16;
         bytes = (bytes + 255) & ~size_t(255);
         if (budget && in_use + bytes > budget)
             throw Error(DCX_ERR_BUDGET, "device footprint above the context budget");
         void* p = nullptr;
-        cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, stream) : cudaMallocAsync(&p, bytes, stream);
+        cudaMemPool_t from = (io && io_pool) ? io_pool : pool;
+        cudaError_t e = from ? cudaMallocFromPoolAsync(&p, bytes, from, stream) : cudaMallocAsync(&p, bytes, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw Error(DCX_ERR_OOM, "cudaMallocAsync failed for " + std::to_string(bytes) + " bytes");
@@ -286,6 +293,10 @@ struct Ctx {
 template <typename T>
 DBuf<T>::DBuf(Ctx* ctx, size_t count) : c(ctx), n(count) {
     p = static_cast<T*>(ctx->alloc(count * sizeof(T)));
+}
+template <typename T>
+DBuf<T>::DBuf(Ctx* ctx, size_t count, bool io) : c(ctx), n(count) {
+    p = static_cast<T*>(ctx->alloc(count * sizeof(T), io));
 }
 template <typename T>
 DBuf<T>& DBuf<T>::operator=(DBuf&& o) noexcept {
@@ -617,7 +628,8 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         const uint32_t fill = std::min<uint32_t>(P0, max_chars_in_bits_k(B, 8 * bytes, K));
         P0 = std::max(P, fill);
     }
-    if (c.opt.prefix_chars && depth == 0) P0 = std::min<uint32_t>(L, c.opt.prefix_chars);
+    if (c.opt.prefix_chars && depth == 0)  // forced prefix, within the 3 key words a sort takes
+        P0 = std::min<uint32_t>({L, c.opt.prefix_chars, max_chars_in_bits_k(B, 96, K)});
     if (P0 == 0) P0 = 1;
     KeyPlan plan = make_plan(B, P0, K);  // key = text id * B^P0 + window
     if (plan.kw > 3) throw Error(DCX_ERR_INTERNAL, "prefix key wider than 3 words");
@@ -1279,11 +1291,11 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     DBuf<uint8_t> t_in;
     const uint8_t* dtext = text;
     if (dev && ((uintptr_t)text & 15)) {  // the byte kernels load 16 bytes at a time
-        t_in = DBuf<uint8_t>(&c, n + 16);
+        t_in = DBuf<uint8_t>(&c, n + 16, true);
         DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyDeviceToDevice, c.stream));
         dtext = t_in.get();
     } else if (!dev) {
-        t_in = DBuf<uint8_t>(&c, n + 16);
+        t_in = DBuf<uint8_t>(&c, n + 16, true);
         DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyHostToDevice, c.stream));
         dtext = t_in.get();
     }
@@ -1347,7 +1359,7 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     DBuf<uint8_t> stage;
     void* dout = sa_out;
     if (!dev || ((uintptr_t)sa_out & 15)) {
-        stage = DBuf<uint8_t>(&c, n * wb + 16);
+        stage = DBuf<uint8_t>(&c, n * wb + 16, true);
         dout = stage.get();
     }
     if (wide_text) {
@@ -1437,7 +1449,7 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
         DBuf<uint8_t> din;
         const uint8_t* dsrc = texts + (offsets[s0] - base0);
         if (!dev) {
-            din = DBuf<uint8_t>(&c, in_bytes + 16);
+            din = DBuf<uint8_t>(&c, in_bytes + 16, true);
             if (in_bytes) DCX_CUDA(cudaMemcpyAsync(din.get(), dsrc, in_bytes, cudaMemcpyHostToDevice, c.stream));
             dsrc = din.get();
         }
@@ -1496,7 +1508,7 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
         DBuf<uint8_t> rstage;
         uint8_t* rout = (uint8_t*)sa_out + (offsets[s0] - base0) * wb;
         if (!dev) {
-            rstage = DBuf<uint8_t>(&c, std::max<uint64_t>(in_bytes, 1) * wb + 16);
+            rstage = DBuf<uint8_t>(&c, std::max<uint64_t>(in_bytes, 1) * wb + 16, true);
             rout = rstage.get();
         }
         auto run_group = [&](const Segs& g, const std::vector<uint32_t>& ids) {
@@ -1643,6 +1655,12 @@ static void ctx_init(Ctx& c, int device, uint64_t budget) {
     DCX_CUDA(cudaMemset(c.d_err, 0, 4));
     DCX_CUDA(cudaMalloc(&c.d_h256, 256 * 8));
     DCX_CUDA(cudaHostAlloc((void**)&c.h_pinned, PINNED_WORDS * 4, cudaHostAllocDefault));
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    DCX_CUDA(cudaMemPoolCreate(&c.io_pool, &props));
+    DCX_CUDA(cudaMemPoolSetAttribute(c.io_pool, cudaMemPoolAttrReleaseThreshold, &thr));
 }
 
 static void ctx_free(Ctx& c) {
@@ -1658,6 +1676,8 @@ static void ctx_free(Ctx& c) {
     for (auto& kv : c.dc_dev) cudaFree(kv.second);
     for (auto& kv : c.dc_flags_dev) cudaFree(kv.second);
     if (c.stream) cudaStreamDestroy(c.stream);
+    if (c.io_pool) cudaMemPoolDestroy(c.io_pool);
+    c.io_pool = nullptr;
     c.stream = nullptr;
     c.d_lookback = nullptr;
     c.h_pinned = nullptr;
