@@ -1611,7 +1611,8 @@ static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
         dsa = sa_in.get();
     }
     DBuf<uint32_t> phi(&c, n), sa32(&c, n), plcp(&c, n);
-    k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(dsa, sa_width, n, phi.get(), sa32.get());
+    k_sa_to_u32<<<grid_for(div_up(n, 4), 256), 256, 0, c.stream>>>(dsa, sa_width, n, sa32.get());
+    k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, phi.get());
     DCX_CHECK_LAUNCH();
     sa_in.reset();
     k_plcp<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(t.get(), n, phi.get(), plcp.get());
@@ -1626,7 +1627,7 @@ static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     k_lcp_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), plcp.get(), n, dout, lcp_width,
                                                         (flags & DCX_LCP_PERMUTED) != 0);
     DCX_CHECK_LAUNCH();
-    c.launched(3);
+    c.launched(4);
     if (!dev) DCX_CUDA(cudaMemcpyAsync(out, dout, n * lb, cudaMemcpyDeviceToHost, c.stream));
     DCX_CUDA(cudaStreamSynchronize(c.stream));
 }

@@ -23,14 +23,29 @@ __device__ __forceinline__ uint64_t load_sa_u(const void* sa, uint64_t k, int wi
            ((uint64_t)b[4] << 32);
 }
 
-// phi[SA[k]] = SA[k-1] (PHI_NONE for k = 0); sa32 receives the SA as uint32.
-__global__ void k_phi(const void* __restrict__ sa, int width, uint64_t n, uint32_t* __restrict__ phi,
-                      uint32_t* __restrict__ sa32) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = (uint32_t)load_sa_u(sa, k, width);
-        sa32[k] = s;
-        phi[s] = k ? (uint32_t)load_sa_u(sa, k - 1, width) : PHI_NONE;
+// The SA as uint32 (coalesced: 40-bit entries are read four at a time as five
+// aligned words when the buffer is 4-byte aligned).
+__global__ void k_sa_to_u32(const void* __restrict__ sa, int width, uint64_t n, uint32_t* __restrict__ sa32) {
+    const bool quad40 = width == 40 && ((uintptr_t)sa & 3) == 0;
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q * 4 < n; q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k0 = q * 4;
+        if (quad40 && k0 + 4 <= n) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(sa) + q * 5;  // 20 bytes = 4 entries
+            const uint32_t w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+            sa32[k0] = w0;                             // bytes 0-3 (byte 4 is the high byte, 0 here)
+            sa32[k0 + 1] = (w1 >> 8) | (w2 << 24);     // bytes 5-8
+            sa32[k0 + 2] = (w2 >> 16) | (w3 << 16);    // bytes 10-13
+            sa32[k0 + 3] = (w3 >> 24) | (w[4] << 8);   // bytes 15-18
+        } else {
+            for (uint64_t k = k0; k < k0 + 4 && k < n; k++) sa32[k] = (uint32_t)load_sa_u(sa, k, width);
+        }
     }
+}
+
+// phi[SA[k]] = SA[k-1] (PHI_NONE for k = 0).
+__global__ void k_phi(const uint32_t* __restrict__ sa32, uint64_t n, uint32_t* __restrict__ phi) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        phi[sa32[k]] = k ? sa32[k - 1] : PHI_NONE;
 }
 
 // 8 chars starting at p from a text padded with at least 8 readable bytes past
