@@ -646,11 +646,6 @@ __global__ void k_emit_seg(const uint32_t* __restrict__ sa_full, const uint32_t*
     }
 }
 
-__global__ void k_widen(const uint32_t* __restrict__ sa, uint64_t n, uint8_t* __restrict__ out, int width) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
-        store_sa_entry(out, k, sa[k], width);
-}
-
 // ---- suffix-array checker (the conditions of check_suffixarray,
 // lightweight_dcx/src/sa_check.hpp:56-184, without its sorts) ------------------
 __device__ __forceinline__ uint64_t load_sa_entry(const void* sa, uint64_t k, int width) {
