@@ -1,0 +1,48 @@
+"""Committed fixtures (tests/golden/sa_lcp_fixtures.npz, made by
+tests/golden/make_golden.py from libsais compiled out of the reference tree):
+the CPU restatement of PDCX reproduces every fixture SA (CPU), and the GPU
+build and LCP reproduce them through the C ABI (GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sa_lcp_fixtures.npz")
+
+
+def _fixtures():
+    with np.load(FIX) as z:
+        names = sorted(k[len("text_"):] for k in z.files if k.startswith("text_"))
+        return [(n, z["text_" + n], z["sa_" + n].astype(np.uint64), z["lcp_" + n].astype(np.uint64)) for n in names]
+
+
+def test_fixture_set_is_complete():
+    fx = _fixtures()
+    assert len(fx) == 11
+    for name, t, sa, lcp in fx:
+        assert sa.size == t.size == lcp.size, name
+        assert np.array_equal(np.sort(sa), np.arange(t.size, dtype=np.uint64)), name
+
+
+@pytest.mark.parametrize("dc", [3, 39])
+def test_restatement_matches_fixtures(oracle, dc):
+    for name, t, sa, _ in _fixtures():
+        if int(t.max(initial=1)) == 255 and np.unique(t).size == 256:
+            continue  # the reference cli refuses 256 symbols; the restatement follows it
+        assert np.array_equal(oracle.dcx_sa(t, X=dc).astype(np.uint64), sa), (name, dc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dc,width", [(3, 64), (7, 32), (13, 40), (39, 40), (39, 64)])
+def test_gpu_sa_matches_fixtures(ctx, dc, width):
+    for name, t, sa, _ in _fixtures():
+        assert np.array_equal(ctx.build_sa(t, dc=dc, sa_width=width), sa), (name, dc, width)
+
+
+@pytest.mark.gpu
+def test_gpu_batch_and_lcp_match_fixtures(ctx):
+    fx = _fixtures()
+    got = ctx.build_sa_batch([t for _, t, _, _ in fx], dc=0, sa_width=32)
+    for (name, t, sa, lcp), g in zip(fx, got):
+        assert np.array_equal(g, sa), name
+        assert np.array_equal(ctx.build_lcp(t, sa), lcp), name
