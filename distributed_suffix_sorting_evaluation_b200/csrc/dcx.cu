@@ -400,7 +400,11 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
     for (uint32_t p = 0; p < passes; p++) {
         const uint32_t* hp = &h[(size_t)p * RADIX];
         uint32_t mx = *std::max_element(hp, hp + RADIX);
-        if ((uint64_t)mx == count) continue;
+        uint64_t sum = 0;
+        for (int d = 0; d < RADIX; d++) sum += hp[d];
+        // one digit value for all keys, or a digit the producer left uncounted
+        // because it is zero in every key
+        if ((uint64_t)mx == count || sum == 0) continue;
         run.push_back(p);
         uint32_t acc = 0;
         for (int d = 0; d < RADIX; d++) {
@@ -660,16 +664,17 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
             uint64_t pow_top = 1;
             for (uint32_t i = 1; i < P0; i++) pow_top *= B;
             const uint64_t seg_mul = pow_top * B;  // B^P0: weight of the text id digit
+            const uint32_t nbytes = (key_bits_k(B, P0, K) + 7) / 8;  // digit bytes that can be nonzero
             const size_t sshm = keys_slide_smem<CharT>();
             const int sgrid = (int)std::min<uint64_t>(div_up(N, SLIDE_TILE), 148 * 3);  // 3 CTAs per SM by smem
             if (SEGK) {
                 DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<true, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
                 k_keys_slide<true, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, seg_mul,
-                                                                                    ko, s.v[0], c.d_hist);
+                                                                                    ko, s.v[0], c.d_hist, nbytes);
             } else {
                 DCX_CUDA(cudaFuncSetAttribute(k_keys_slide<false, CharT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sshm));
                 k_keys_slide<false, CharT><<<sgrid, SLIDE_THREADS, sshm, c.stream>>>(text, N, sv, plan, pow_top, seg_mul,
-                                                                                     ko, s.v[0], c.d_hist);
+                                                                                     ko, s.v[0], c.d_hist, nbytes);
             }
         } else {
 #define DCX_PREFIX(KWV, SEGV)                                                                                       \

@@ -75,12 +75,14 @@ struct KeyOut {
 constexpr int HIST_COPIES = 4;
 
 template <int KW>
-__device__ __forceinline__ void hist_add(uint32_t* sh, const uint32_t* key) {
+__device__ __forceinline__ void hist_add(uint32_t* sh, const uint32_t* key, uint32_t nbytes = 4 * KW) {
     uint32_t* h = sh + (threadIdx.x >> 6) * (4 * KW * RADIX);
 #pragma unroll
     for (int w = 0; w < KW; w++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) atomicAdd(&h[(4 * w + b) * RADIX + ((key[w] >> (8 * b)) & (RADIX - 1))], 1u);
+        for (int b = 0; b < 4; b++)
+            if ((uint32_t)(4 * w + b) < nbytes)  // higher digit bytes are zero by construction
+                atomicAdd(&h[(4 * w + b) * RADIX + ((key[w] >> (8 * b)) & (RADIX - 1))], 1u);
 }
 
 // Zero the private copies / fold them into the global histogram.
@@ -160,7 +162,7 @@ template <bool SEG, typename CharT>
 __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __restrict__ text, uint64_t N, SegView sv,
                                                               KeyPlan plan, uint64_t pow_top, uint64_t seg_mul,
                                                               KeyOut ko, uint32_t* __restrict__ vals_out,
-                                                              uint32_t* hist) {
+                                                              uint32_t* hist, uint32_t nbytes) {
     extern __shared__ uint32_t sh[];  // HIST_COPIES * 8 * RADIX histogram words, then the staging area
     uint32_t* hst = sh;
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(sh + HIST_COPIES * 8 * RADIX);  // SLIDE_TILE keys, padded
@@ -209,8 +211,8 @@ __global__ __launch_bounds__(SLIDE_THREADS) void k_keys_slide(const CharT* __res
             ko.w[0][base + i] = kk[0];
             if (W > 1) ko.w[1][base + i] = kk[1];
             vals_out[base + i] = (uint32_t)(base + i);
-            if (W == 2) hist_add<2>(hst, kk);
-            else hist_add<1>(hst, kk);
+            if (W == 2) hist_add<2>(hst, kk, nbytes);
+            else hist_add<1>(hst, kk, nbytes);
         }
         __syncthreads();
     }
