@@ -555,41 +555,42 @@ static RefinePlan8 make_refine8(uint64_t B, uint32_t P) {
     return r8;
 }
 
-template <int C, int T, int W>
-static void launch_refine_seg(Ctx& c, const uint8_t* text, SegView sv, const uint32_t* segw, const uint32_t* gstart,
+template <int C, int T, int W, typename CharT>
+static void launch_refine_seg(Ctx& c, const CharT* text, SegView sv, const uint32_t* segw, const uint32_t* gstart,
                               const uint32_t* gsize, uint64_t ng, uint32_t* sa, uint8_t* head,
                               const RefineSegPlan& plan) {
     const size_t shm = refine_seg_smem<C, W>();
-    DCX_CUDA(cudaFuncSetAttribute(k_refine_seg<C, T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    auto kern = k_refine_seg<C, T, W, CharT>;
+    DCX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     int per_sm = 0;
-    DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_seg<C, T, W>, T, shm));
+    DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, shm));
     const uint64_t grid = std::min<uint64_t>(ng, 148ull * std::max(per_sm, 1));
-    k_refine_seg<C, T, W><<<(unsigned)grid, T, shm, c.stream>>>(text, sv, segw, gstart, gsize, ng, sa, head, plan);
+    kern<<<(unsigned)grid, T, shm, c.stream>>>(text, sv, segw, gstart, gsize, ng, sa, head, plan);
     DCX_CHECK_LAUNCH();
     c.launched();
 }
 
 // Groups of two (class 0) and of 3..32 (classes 1-4).
-template <int W>
-static void refine_small_w(Ctx& c, const uint8_t* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
+template <int W, typename CharT>
+static void refine_small_w(Ctx& c, const CharT* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
                            uint32_t* sa, uint8_t* head, const RefineSegPlan& plan) {
     if (tg.counts[0]) {
-        k_refine_pair<W><<<grid_for(tg.counts[0], 256, 148 * 16), 256, 0, c.stream>>>(
+        k_refine_pair<W, CharT><<<grid_for(tg.counts[0], 256, 148 * 16), 256, 0, c.stream>>>(
             text, sv, segw, tg.gstart.get(), tg.counts[0], sa, head, plan);
         DCX_CHECK_LAUNCH();
         c.launched();
     }
     const uint64_t g0 = tg.off[1], ng = tg.off[5] - g0;
     if (ng) {
-        k_refine_warp<W><<<grid_for(ng * 32, 256, 148 * 16), 256, 0, c.stream>>>(
+        k_refine_warp<W, CharT><<<grid_for(ng * 32, 256, 148 * 16), 256, 0, c.stream>>>(
             text, sv, segw, tg.gstart.get() + g0, tg.gsize.get() + g0, ng, sa, head, plan);
         DCX_CHECK_LAUNCH();
         c.launched();
     }
 }
 
-template <int C, int T>
-static void refine_seg_class(Ctx& c, const uint8_t* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
+template <int C, int T, typename CharT>
+static void refine_seg_class(Ctx& c, const CharT* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
                              int cls_lo, int cls_hi, uint32_t* sa, uint8_t* head, const RefineSegPlan& plan) {
     const uint64_t g0 = tg.off[cls_lo], ng = tg.off[cls_hi + 1] - g0;
     if (!ng) return;
@@ -599,7 +600,9 @@ static void refine_seg_class(Ctx& c, const uint8_t* text, SegView sv, const uint
         case 1: launch_refine_seg<C, T, 1>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
         case 2: launch_refine_seg<C, T, 2>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
         case 3: launch_refine_seg<C, T, 3>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
-        default: launch_refine_seg<C, T, 4>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+        case 4: launch_refine_seg<C, T, 4>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+        case 5: launch_refine_seg<C, T, 5>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
+        default: launch_refine_seg<C, T, 6>(c, text, sv, segw, gs, gz, ng, sa, head, plan); break;
     }
 }
 
@@ -717,11 +720,12 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     uint8_t* hd = head.get();  // head flags the global rounds work on
     TieGroups tg;
     DBuf<uint8_t> head2;
-    if (covered < L && sizeof(CharT) == 1 && B <= 256 && ((uintptr_t)text & 7) == 0) {
+    const bool seg_chars = sizeof(CharT) == 1 ? (B <= 256 && ((uintptr_t)text & 7) == 0) : true;
+    if (covered < L && seg_chars && B <= 0xffffffffull) {
         // Groups of up to 2048 elements are sorted by the whole rest of the window
         // inside one CTA each; only larger groups take the global radix rounds.
         const uint32_t rem = L - covered;
-        const uint32_t cpw = std::min<uint32_t>(64, max_chars_in_bits(B, 64));
+        const uint32_t cpw = std::min<uint32_t>(sizeof(CharT) == 1 ? 64 : 16, max_chars_in_bits(B, 64));
         const uint32_t W = (rem + cpw - 1) / cpw;
         if (W <= (uint32_t)RSEG_MAX_W) {
             tg = group_ties(c, hd, N);
@@ -731,13 +735,15 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
                 plan.off[w] = covered + w * cpw;
                 plan.rp[w] = make_refine8(B, std::min(cpw, rem - w * cpw));
             }
-            const uint8_t* t8 = reinterpret_cast<const uint8_t*>(text);
+            const CharT* t8 = text;
             const uint32_t* sw = SEGK ? segw.get() : nullptr;
             switch (W) {
                 case 1: refine_small_w<1>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
                 case 2: refine_small_w<2>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
                 case 3: refine_small_w<3>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
-                default: refine_small_w<4>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+                case 4: refine_small_w<4>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+                case 5: refine_small_w<5>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
+                default: refine_small_w<6>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
             }
             refine_seg_class<64, 32>(c, t8, sv, sw, tg, 5, 5, sa.get(), hd, plan);
             refine_seg_class<256, 128>(c, t8, sv, sw, tg, 6, 7, sa.get(), hd, plan);

@@ -325,6 +325,20 @@ __device__ __forceinline__ uint64_t window_value8(const uint64_t* __restrict__ t
     return key;
 }
 
+// Window value for the segmented refinement: byte texts use the SWAR word
+// loader, 32-bit texts (alphabet of 256 symbols) fold rp.P chars directly.
+__device__ __forceinline__ uint64_t window_value_t(const uint8_t* t, uint64_t s, uint64_t end, const RefinePlan8& rp) {
+    return window_value8(reinterpret_cast<const uint64_t*>(t), s, end, rp);
+}
+__device__ __forceinline__ uint64_t window_value_t(const uint32_t* t, uint64_t s, uint64_t end, const RefinePlan8& rp) {
+    uint64_t k = 0;
+    for (uint32_t j = 0; j < rp.P; j++) {
+        const uint64_t p = s + j;
+        k = k * rp.B + (p < end ? __ldg(t + p) : 0u);
+    }
+    return k;
+}
+
 template <int KW>
 __global__ __launch_bounds__(256) void k_keys_refine8(const uint8_t* __restrict__ text, SegView sv, uint64_t count,
                                                       const uint32_t* __restrict__ tpos,
@@ -358,15 +372,15 @@ __global__ __launch_bounds__(256) void k_keys_refine8(const uint8_t* __restrict_
 // the group is written back with head flags where the words change.  Equal
 // windows stay tied (head 0) for the cover-rank tie break.  The CTA loops over
 // groups.
-constexpr int RSEG_MAX_W = 4;
+constexpr int RSEG_MAX_W = 6;
 struct RefineSegPlan {
     uint32_t W;                       // words per element
     uint32_t off[RSEG_MAX_W];         // first char of each word, relative to the position
     RefinePlan8 rp[RSEG_MAX_W];
 };
 
-template <int C, int THREADS, int W>
-__global__ __launch_bounds__(THREADS) void k_refine_seg(const uint8_t* __restrict__ text, SegView sv,
+template <int C, int THREADS, int W, typename CharT>
+__global__ __launch_bounds__(THREADS) void k_refine_seg(const CharT* __restrict__ text, SegView sv,
                                                         const uint32_t* __restrict__ segw,
                                                         const uint32_t* __restrict__ gstart,
                                                         const uint32_t* __restrict__ gsize, uint64_t ngroups,
@@ -377,7 +391,6 @@ __global__ __launch_bounds__(THREADS) void k_refine_seg(const uint8_t* __restric
     uint64_t(*s_key)[C] = reinterpret_cast<uint64_t(*)[C]>(s_dyn64);             // [W][C]
     uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_dyn64 + (size_t)W * C);      // [C]
     uint16_t* s_idx = reinterpret_cast<uint16_t*>(s_pos + C);                    // [C]
-    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
     for (uint64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const uint32_t start = gstart[g], size = gsize[g];
         const uint64_t end = seg_end(sv, segw ? segw[start] : 0u);
@@ -387,7 +400,7 @@ __global__ __launch_bounds__(THREADS) void k_refine_seg(const uint8_t* __restric
                 const uint32_t p = sa[start + i];
                 s_pos[i] = p;
 #pragma unroll
-                for (int w = 0; w < W; w++) s_key[w][i] = window_value8(tw0, (uint64_t)p + plan.off[w], end, plan.rp[w]);
+                for (int w = 0; w < W; w++) s_key[w][i] = window_value_t(text, (uint64_t)p + plan.off[w], end, plan.rp[w]);
             }
         }
         __syncthreads();
@@ -434,13 +447,12 @@ __global__ __launch_bounds__(THREADS) void k_refine_seg(const uint8_t* __restric
 }
 
 // Groups of exactly two: one thread per group.
-template <int W>
-__global__ __launch_bounds__(256) void k_refine_pair(const uint8_t* __restrict__ text, SegView sv,
+template <int W, typename CharT>
+__global__ __launch_bounds__(256) void k_refine_pair(const CharT* __restrict__ text, SegView sv,
                                                      const uint32_t* __restrict__ segw,
                                                      const uint32_t* __restrict__ gstart, uint64_t ngroups,
                                                      uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
                                                      RefineSegPlan plan) {
-    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
     for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t start = gstart[g];
@@ -450,8 +462,8 @@ __global__ __launch_bounds__(256) void k_refine_pair(const uint8_t* __restrict__
 #pragma unroll
         for (int w = 0; w < W; w++) {
             if (cmp) break;
-            const uint64_t ka = window_value8(tw0, (uint64_t)a + plan.off[w], end, plan.rp[w]);
-            const uint64_t kb = window_value8(tw0, (uint64_t)b + plan.off[w], end, plan.rp[w]);
+            const uint64_t ka = window_value_t(text, (uint64_t)a + plan.off[w], end, plan.rp[w]);
+            const uint64_t kb = window_value_t(text, (uint64_t)b + plan.off[w], end, plan.rp[w]);
             cmp = ka < kb ? -1 : (ka > kb ? 1 : 0);
         }
         if (cmp > 0) {
@@ -464,14 +476,13 @@ __global__ __launch_bounds__(256) void k_refine_pair(const uint8_t* __restrict__
 
 // Groups of 3..32 elements: one warp per group, one element per lane, a
 // bitonic network over the lanes with shuffles.
-template <int W>
-__global__ __launch_bounds__(256) void k_refine_warp(const uint8_t* __restrict__ text, SegView sv,
+template <int W, typename CharT>
+__global__ __launch_bounds__(256) void k_refine_warp(const CharT* __restrict__ text, SegView sv,
                                                      const uint32_t* __restrict__ segw,
                                                      const uint32_t* __restrict__ gstart,
                                                      const uint32_t* __restrict__ gsize, uint64_t ngroups,
                                                      uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
                                                      RefineSegPlan plan) {
-    const uint64_t* tw0 = reinterpret_cast<const uint64_t*>(text);
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += warps) {
@@ -481,7 +492,7 @@ __global__ __launch_bounds__(256) void k_refine_warp(const uint8_t* __restrict__
         uint32_t p = valid ? sa[start + lane] : 0u;
         uint64_t key[W];
 #pragma unroll
-        for (int w = 0; w < W; w++) key[w] = valid ? window_value8(tw0, (uint64_t)p + plan.off[w], end, plan.rp[w]) : 0ull;
+        for (int w = 0; w < W; w++) key[w] = valid ? window_value_t(text, (uint64_t)p + plan.off[w], end, plan.rp[w]) : 0ull;
 #pragma unroll
         for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
