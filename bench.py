@@ -791,7 +791,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--text-mib", type=int, default=0, help="override the text size (profiling captures)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample-mib", type=int, default=256)
     ap.add_argument("--ref-sample-mib", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
