@@ -1299,16 +1299,20 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     cudaEventCreate(&e2);
     cudaEventCreate(&e3);
     cudaEventRecord(e0, c.stream);
-    DBuf<uint8_t> t_in;
+    // Staging (host-pointer calls; device buffers the byte kernels cannot use in
+    // place) is ONE allocation of the same size every call, so the staging pool
+    // reuses it instead of splitting blocks: text copy first, then the SA.
+    const size_t wb = width / 8;
+    const bool stage_text = !dev || ((uintptr_t)text & 15);  // the byte kernels load 16 bytes at a time
+    const bool stage_sa = !dev || ((uintptr_t)sa_out & 15);
+    const size_t text_region = stage_text ? ((n + 16 + 255) & ~size_t(255)) : 0;
+    DBuf<uint8_t> io;
+    if (stage_text || stage_sa) io = DBuf<uint8_t>(&c, text_region + (stage_sa ? n * wb + 16 : 0), true);
     const uint8_t* dtext = text;
-    if (dev && ((uintptr_t)text & 15)) {  // the byte kernels load 16 bytes at a time
-        t_in = DBuf<uint8_t>(&c, n + 16, true);
-        DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyDeviceToDevice, c.stream));
-        dtext = t_in.get();
-    } else if (!dev) {
-        t_in = DBuf<uint8_t>(&c, n + 16, true);
-        DCX_CUDA(cudaMemcpyAsync(t_in.get(), text, n, cudaMemcpyHostToDevice, c.stream));
-        dtext = t_in.get();
+    if (stage_text) {
+        DCX_CUDA(cudaMemcpyAsync(io.get(), text, n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 c.stream));
+        dtext = io.get();
     }
     cudaEventRecord(e1, c.stream);
     // phase 0: alphabet (compress_alphabet, cli.cpp:417-463)
@@ -1366,13 +1370,7 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     one.start = {0, n + 1};
     DCX_CUDA(cudaMemsetAsync(t_map.get() + n, 0, 16, c.stream));
     // SA straight into the caller's device buffer, or into a staging buffer for host pointers
-    const size_t wb = width / 8;
-    DBuf<uint8_t> stage;
-    void* dout = sa_out;
-    if (!dev || ((uintptr_t)sa_out & 15)) {
-        stage = DBuf<uint8_t>(&c, n * wb + 16, true);
-        dout = stage.get();
-    }
+    void* dout = stage_sa ? (void*)(io.get() + text_region) : sa_out;
     if (wide_text) {
         // all 256 byte values occur: remap b -> b + 1 into 32-bit chars and build
         // with 257-symbol keys (the reference cli refuses this input)
@@ -1381,11 +1379,9 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         k_widen_text<<<grid_for(n, 256), 256, 0, c.stream>>>(dtext, n, t32.get());
         DCX_CHECK_LAUNCH();
         c.launched();
-        t_in.reset();
         t_map.reset();
         level<uint32_t>(c, t32.get(), one, sigma, (uint32_t)X, 0, packing, dout, width);
     } else {
-        t_in.reset();
         level<uint8_t>(c, t_map.get(), one, sigma, (uint32_t)X, 0, packing, dout, width);
     }
     t_map.reset();
