@@ -50,6 +50,19 @@ def test_null_context_rejected():
     lib = pkg.load_library()
     assert lib.dcx_build_sa(None, None, 0, 39, 40, None, 0) == pkg.DCX_ERR_ARG
     assert lib.dcx_ctx_destroy(None) == pkg.DCX_ERR_ARG
+    # every other context call checks its context before touching a device
+    rid = ctypes.c_uint64()
+    st = ctypes.c_int()
+    ok = ctypes.c_int()
+    assert lib.dcx_build_sa_batch(None, None, None, 0, 0, 32, None, 0) == pkg.DCX_ERR_ARG
+    assert lib.dcx_build_lcp(None, None, 0, None, 32, None, 32, 0) == pkg.DCX_ERR_ARG
+    assert lib.dcx_check_sa(None, None, 0, None, 32, 0, ctypes.byref(ok)) == pkg.DCX_ERR_ARG
+    assert lib.dcx_serve_submit(None, None, 0, 0, 32, ctypes.byref(rid)) == pkg.DCX_ERR_ARG
+    assert lib.dcx_serve_submit_ex(None, None, 0, 0, 32, 0, ctypes.byref(rid)) == pkg.DCX_ERR_ARG
+    assert lib.dcx_serve_poll(None, 1, None, ctypes.byref(st), None) == pkg.DCX_ERR_ARG
+    assert lib.dcx_serve_release(None, 1) == pkg.DCX_ERR_ARG
+    assert lib.dcx_serve_drain(None) == pkg.DCX_ERR_ARG
+    assert lib.dcx_set_option(None, b"trace", 1.0) == pkg.DCX_ERR_ARG
 
 
 def test_uint40_unpacking():
