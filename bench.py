@@ -46,6 +46,18 @@ def _dist():
     return world, rank, local
 
 
+def max_over_ranks(value: float, world: int, device="cpu") -> float:
+    """Largest value over the ranks of the process group (the job's time is its
+    slowest rank's); the value itself when running alone.  `device` is where the
+    backend reduces: the rank's GPU for NCCL, "cpu" for gloo."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -303,10 +315,7 @@ def run_gpu(args, world, rank, local):
         verified = ctx.check_sa_device(d_text.data_ptr(), n, d_sa.data_ptr(), width)
         if not verified:
             raise SystemExit("the suffix array failed the GPU check")
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, f"cuda:{local}")
     ms_step = ms / args.steps
     value = world * n / GiB / (ms_step / 1000.0)
 
@@ -350,10 +359,7 @@ def run_gpu(args, world, rank, local):
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms_e2e = statistics.median(step_ms)
     e2e_stats = ctx.stats()
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, world, f"cuda:{local}")
     e2e_value = world * n / GiB / (ms_e2e / 1000.0)
     e2e_mean = world * n / GiB / (sum(step_ms) / len(step_ms) / 1000.0)
 
@@ -513,10 +519,7 @@ def run_batch(args, world, rank, local):
                 loop_open = loop_ms < args.loop_budget_s * 1000.0
     clock = clocks.summary()
     ms_total = sum(batch_ms)
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(ms_total, world, dev)
     value = world * total / GiB / (ms_total / 1000.0)
     if rank == 0:
         loop_v = loop_bytes / GiB / (loop_ms / 1000.0) if loop_ms > 0 else None
