@@ -415,28 +415,24 @@ def run_gpu(args, world, rank, local):
     return 0
 
 
-def run_batch(args, world, rank, local):
-    """Batched workload: `count` independent i.i.d. {A,C,G,T} texts, lengths
-    log-uniform in [1 KiB, 16 MiB] (seeded), one uint32 SA per text.  The texts
-    are staged on the device a chunk (about --batch-chunk-mib of text) at a time;
-    the timed region is the batched call over every chunk with the chunk's text
-    already in HBM.  Beside it, the plain single-text call is looped over the
-    same texts (whole chunks, while --loop-budget-s lasts) and the batched time
-    of exactly those chunks gives the speed-up.  Under torchrun every rank runs
-    its own copy of the batch (replicas)."""
-    import torch
-    from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
+def batch_share(lens, world, rank, cap, split="lpt"):
+    """This rank's part of the batched workload: (indices of its texts in batch
+    order, seed offset of its texts, bytes the whole job builds, chunks of the
+    rank with the most chunks).  "lpt" splits the texts by size, longest first
+    (every rank computes the same split, no collective); "replicas" gives every
+    rank all texts with its own seeds.  Every rank steps through the largest
+    chunk count so that all ranks enter the same barriers."""
+    if world <= 1 or split == "replicas":
+        shift = 7919 * rank if world > 1 else 0
+        return np.arange(lens.size), shift, world * int(lens.sum()), len(batch_chunks(lens, cap))
+    from distributed_suffix_sorting_evaluation_b200 import shard_texts
+    owner, _ = shard_texts(lens, world)
+    steps = max(len(batch_chunks(lens[owner == r], cap)) for r in range(world))
+    return np.flatnonzero(owner == rank), 0, int(lens.sum()), steps
 
-    torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    dev = f"cuda:{local}"
-    lens = W.batch_lengths(args.batch_count, 1 << 10, 16 << 20, seed=5)
-    total = int(lens.sum())
-    # chunks of consecutive texts, each about batch_chunk_mib of text
-    cap = args.batch_chunk_mib << 20
+
+def batch_chunks(lens, cap):
+    """Consecutive runs of texts of about `cap` bytes each: (first, end, bytes)."""
     chunks, s0 = [], 0
     while s0 < lens.size:
         s1, tot = s0, 0
@@ -445,6 +441,37 @@ def run_batch(args, world, rank, local):
             s1 += 1
         chunks.append((s0, s1, tot))
         s0 = s1
+    return chunks
+
+
+def run_batch(args, world, rank, local):
+    """Batched workload: `count` independent i.i.d. {A,C,G,T} texts, lengths
+    log-uniform in [1 KiB, 16 MiB] (seeded), one uint32 SA per text.  The texts
+    are staged on the device a chunk (about --batch-chunk-mib of text) at a time;
+    the timed region is the batched call over every chunk with the chunk's text
+    already in HBM.  Beside it, the plain single-text call is looped over the
+    same texts (whole chunks, while --loop-budget-s lasts) and the batched time
+    of exactly those chunks gives the speed-up.  Under torchrun the texts are
+    split over the ranks by size, longest first (--batch-split lpt, strong
+    scaling: the same 20,000 texts in total), or every rank builds its own
+    copy of the batch (--batch-split replicas, weak scaling)."""
+    import torch
+    from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
+
+    if args.batch_count < world:
+        raise SystemExit("the batched workload needs at least one text per rank")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    all_lens = W.batch_lengths(args.batch_count, 1 << 10, 16 << 20, seed=5)
+    ids, seed_shift, job_bytes, nsteps = batch_share(all_lens, world, rank, args.batch_chunk_mib << 20,
+                                                     args.batch_split)
+    lens = all_lens[ids]
+    total = int(lens.sum())
+    chunks = batch_chunks(lens, args.batch_chunk_mib << 20)
     big = max(c[2] for c in chunks)
     d_text = torch.empty(big + 16, dtype=torch.uint8, device=dev)
     d_sa = torch.empty(big + 16, dtype=torch.int32, device=dev)
@@ -461,7 +488,7 @@ def run_batch(args, world, rank, local):
         hv = h_text.numpy()
         for j in range(a, b):
             o = int(offs[j - a])
-            W.iid(int(lens[j]), b"ACGT", seed=1_000_000 + j + 7919 * rank, out=hv[o:o + int(lens[j])])
+            W.iid(int(lens[j]), b"ACGT", seed=1_000_000 + int(ids[j]) + seed_shift, out=hv[o:o + int(lens[j])])
         d_text[:tot].copy_(h_text[:tot], non_blocking=True)
         torch.cuda.synchronize()
         return offs
@@ -485,7 +512,10 @@ def run_batch(args, world, rank, local):
     verified = 0
     loop_open = args.loop_budget_s > 0
     with ClockSampler(local) as clocks:
-        for ci in range(len(chunks)):
+        for ci in range(nsteps):
+            if ci >= len(chunks):  # another rank still has chunks: meet its barriers
+                torch.distributed.barrier()
+                continue
             offs = offs0 if ci == 0 else stage(ci)
             if world > 1:
                 torch.distributed.barrier()
@@ -505,7 +535,7 @@ def run_batch(args, world, rank, local):
                     t = h_text.numpy()[o:o + n].copy()
                     raw = d_sa[o:o + n].cpu().numpy().view(np.uint8)
                     if not ctx.check_sa(t, raw, 32):
-                        raise SystemExit(f"batched SA of text {a + k} failed the check")
+                        raise SystemExit(f"batched SA of text {int(ids[a + k])} failed the check")
                     verified += 1
             if loop_open:
                 e0.record(stream)
@@ -520,19 +550,22 @@ def run_batch(args, world, rank, local):
     clock = clocks.summary()
     ms_total = sum(batch_ms)
     ms_total = max_over_ranks(ms_total, world, dev)
-    value = world * total / GiB / (ms_total / 1000.0)
+    value = job_bytes / GiB / (ms_total / 1000.0)
+    split = args.batch_split if world > 1 else "single-gpu"
     if rank == 0:
         loop_v = loop_bytes / GiB / (loop_ms / 1000.0) if loop_ms > 0 else None
         same_v = loop_bytes / GiB / (loop_batch_ms / 1000.0) if loop_batch_ms > 0 else None
         line = {
             "metric": "batched SA build GiB/s", "value": round(value, 4), "unit": "GiB/s", "n_gpus": world,
             "steps": len(chunks), "warmup": max(1, args.warmup), "ms_per_step": round(ms_total / len(chunks), 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "higher_is_better": True, "scaling": "strong" if split == "lpt" else "weak", "vs_baseline": None,
+            "dtype": "u8",
             "data": "synthetic (seeded i.i.d. {A,C,G,T} texts, log-uniform lengths 1 KiB-16 MiB)",
-            "config": {"workload": "cfg4_batch", "texts": int(lens.size), "text_bytes": total,
+            "config": {"workload": "cfg4_batch", "texts": int(all_lens.size), "text_bytes": int(all_lens.sum()),
+                       "job_bytes": int(job_bytes), "rank0_texts": int(lens.size), "rank0_bytes": total,
                        "chunk_mib": args.batch_chunk_mib, "dc": "auto per text", "sa_width": 32,
                        "l2_flush": "each chunk's text and SAs are larger than L2",
-                       "parallelism": "replicas" if world > 1 else "single-gpu"},
+                       "parallelism": split},
             "seconds": round(ms_total / 1000.0, 3),
             "loop": {"value": None if loop_v is None else round(loop_v, 4), "unit": "GiB/s", "texts": loop_texts,
                      "bytes": loop_bytes, "call": "dcx_build_sa per text, DC39, device pointers",
@@ -804,6 +837,8 @@ def main():
                     help="context option (dcx_set_option) for the single-text workloads")
     ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
+    ap.add_argument("--batch-split", default="lpt", choices=["lpt", "replicas"],
+                    help="how the batched workload is split over ranks under torchrun")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")
     ap.add_argument("--verify", action="store_true", help="check the SA (batched: three SAs per chunk) on the GPU")
     ap.add_argument("--serve-requests", type=int, default=20000, help="request pool of the serving workload")

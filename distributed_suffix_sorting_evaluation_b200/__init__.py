@@ -51,7 +51,7 @@ EXPORTED = (
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
-    "dcx_serve_submit_ex", "dcx_build_lcp",
+    "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts",
 )
 
 # serving request states (dcx_serve_poll)
@@ -131,6 +131,7 @@ def load_library(path: str | None = None):
     lib.dcx_build_sa_noalloc.argtypes = [vp, u64, vp, vp]
     lib.dcx_build_lcp.argtypes = [vp, vp, u64, vp, i32, vp, i32, u32]
     lib.dcx_check_sa.argtypes = [vp, vp, u64, vp, i32, u32, ctypes.POINTER(i32)]
+    lib.dcx_shard_texts.argtypes = [vp, u32, u32, vp, vp]
     _lib = lib
     return lib
 
@@ -149,6 +150,20 @@ def dc_table(X: int):
     cmp = np.zeros(X * X * 3, np.uint32)
     _check(lib.dcx_dc_table(X, ctypes.byref(D), dc.ctypes.data, nr.ctypes.data, cmp.ctypes.data))
     return dc[: D.value].copy(), nr, cmp.reshape(X, X, 3)
+
+
+def shard_texts(lengths, world: int):
+    """Size-balanced split of independent texts over `world` ranks, longest
+    first (host-only call): (owner[i] = rank of text i, bytes per rank).  Every
+    rank computes the same split from the same lengths."""
+    lens = np.ascontiguousarray(lengths, dtype=np.uint64)
+    if lens.size >= 1 << 32:
+        raise ValueError("at most 2^32 - 1 texts")
+    owner = np.zeros(lens.size, np.uint32)
+    loads = np.zeros(max(int(world), 0), np.uint64)
+    _check(load_library().dcx_shard_texts(lens.ctypes.data, lens.size, int(world), owner.ctypes.data,
+                                          loads.ctypes.data if loads.size else None))
+    return owner, loads
 
 
 def sa_dtype_bytes(width: int) -> int:

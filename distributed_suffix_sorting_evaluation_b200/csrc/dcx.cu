@@ -1751,6 +1751,30 @@ int dcx_dc_table(int X, uint32_t* D, uint32_t* dc, uint32_t* next_rank, uint32_t
     return DCX_OK;
 }
 
+int dcx_shard_texts(const uint64_t* lengths, uint32_t num_texts, uint32_t world, uint32_t* owner,
+                    uint64_t* load_out) {
+    if (world == 0 || (num_texts > 0 && (!lengths || !owner))) return DCX_ERR_ARG;
+    std::vector<uint32_t> order(num_texts);
+    for (uint32_t i = 0; i < num_texts; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return lengths[a] > lengths[b]; });
+    // min-heap of (load, rank): the lightest rank, the lower rank on equal loads
+    using Slot = std::pair<uint64_t, uint32_t>;
+    std::vector<Slot> heap(world);
+    for (uint32_t r = 0; r < world; ++r) heap[r] = {0, r};
+    auto heavier = [](const Slot& a, const Slot& b) { return a > b; };
+    std::make_heap(heap.begin(), heap.end(), heavier);
+    for (uint32_t i : order) {
+        std::pop_heap(heap.begin(), heap.end(), heavier);
+        owner[i] = heap.back().second;
+        heap.back().first += lengths[i];
+        std::push_heap(heap.begin(), heap.end(), heavier);
+    }
+    if (load_out)
+        for (const Slot& s : heap) load_out[s.second] = s.first;
+    return DCX_OK;
+}
+
 int dcx_ctx_create(dcx_ctx** out, int device, uint64_t budget) {
     if (!out) return DCX_ERR_ARG;
     *out = nullptr;

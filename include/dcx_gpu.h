@@ -146,6 +146,21 @@ int dcx_build_sa_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offse
                        uint32_t num_texts, int dc_or_auto, int sa_width, void* sa_out,
                        uint32_t flags);
 
+/* Splits a batch of independent texts over `world` GPUs, one process per GPU.
+ * The reference splits its single text into equal blocks per rank
+ * (lightweight_dcx/src/mpi/io.hpp:33-65); independent texts need no
+ * exchange, so each rank takes whole texts instead.  Size-balanced, longest
+ * first: texts in order of decreasing length (equal lengths: lower index
+ * first) each go to the rank with the least text so far (equal loads: lower
+ * rank).  owner[i] receives the rank of text i and load_out[r] (may be null)
+ * the bytes of rank r.  The assignment depends only on the lengths, so every
+ * rank computes the same split without a collective; the largest load is at
+ * most 4/3 of the best possible (Graham's bound for longest-first
+ * scheduling).  Host-only, needs no GPU.  DCX_ERR_ARG for world = 0 or null
+ * owner / lengths with num_texts > 0. */
+int dcx_shard_texts(const uint64_t* lengths, uint32_t num_texts, uint32_t world, uint32_t* owner,
+                    uint64_t* load_out);
+
 /* ---- serving (continuous batching) ----------------------------------------- */
 /* No counterpart in the reference (its cli builds one SA per run,
  * cli.cpp:747-820).  A request loop on the context's GPU: requests are copied

@@ -36,6 +36,18 @@ mine = getattr(W, w["gen"])(1 << 16, seed=w["seed"] + 1000 * rank)
 gathered = [None, None]
 dist.all_gather_object(gathered, mine.tobytes()[:4096])
 assert gathered[0] != gathered[1]
+# the batched workload: each rank computes the size-balanced split by itself;
+# together the ranks build every text once and step through the same barriers
+lens = W.batch_lengths(2000, 1 << 10, 16 << 20, seed=5)
+cap = 256 << 20
+ids, shift, job, steps = bench.batch_share(lens, world, rank, cap)
+parts = [None, None]
+dist.all_gather_object(parts, ids.tolist())
+assert sorted(parts[0] + parts[1]) == list(range(lens.size))
+assert shift == 0 and job == int(lens.sum())
+assert steps == max(len(bench.batch_chunks(lens[np.array(p)], cap)) for p in parts)
+ids_r, shift_r, job_r, _ = bench.batch_share(lens, world, rank, cap, "replicas")
+assert ids_r.size == lens.size and shift_r == 7919 * rank and job_r == 2 * int(lens.sum())
 # the reference arm: ranks other than 0 return 0 without output or work
 if rank != 0:
     args = bench.argparse.Namespace(workload=bench.DEFAULT_WORKLOAD, steps=1, warmup=0,
