@@ -334,6 +334,21 @@ def run_gpu(args, world, rank, local):
                     "call": "dcx_build_lcp, device pointers, uint32 LCP"}
         del d_lcp
 
+    bwt_line = None
+    if args.bwt:  # BWT of the built SA, device-resident (primary-index scan + gather)
+        d_bwt = torch.empty(n, dtype=torch.uint8, device=f"cuda:{local}")
+        ctx.build_bwt_device(d_text.data_ptr(), n, d_sa.data_ptr(), width, d_bwt.data_ptr())
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            ctx.build_bwt_device(d_text.data_ptr(), n, d_sa.data_ptr(), width, d_bwt.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_bwt = e0.elapsed_time(e1) / 3
+        bwt_line = {"value": round(n / GiB / (ms_bwt / 1000.0), 4), "unit": "GiB/s", "ms": round(ms_bwt, 3),
+                    "call": "dcx_build_bwt, device pointers"}
+        del d_bwt
+
     # end-to-end through the public call with host buffers; the device-resident
     # buffers of the runs above are released first, so the host-pointer build
     # has the device memory a caller of that path would have
@@ -401,6 +416,8 @@ def run_gpu(args, world, rank, local):
         }
         if lcp_line:
             line["lcp"] = lcp_line
+        if bwt_line:
+            line["bwt"] = bwt_line
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             sample = min(n, args.cpu_sample_mib << 20)
@@ -832,6 +849,7 @@ def main():
     ap.add_argument("--ref-sample-mib", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
+    ap.add_argument("--bwt", action="store_true", help="also time the BWT of the built SA")
     ap.add_argument("--recursion-dc", type=int, default=0, help="difference cover of the recursion levels")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
                     help="context option (dcx_set_option) for the single-text workloads")

@@ -51,7 +51,7 @@ EXPORTED = (
     "dcx_get_stream", "dcx_get_stats", "dcx_get_trace", "dcx_build_sa_batch", "dcx_serve_submit", "dcx_serve_poll",
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
-    "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts",
+    "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
 )
 
 # serving request states (dcx_serve_poll)
@@ -132,6 +132,7 @@ def load_library(path: str | None = None):
     lib.dcx_build_lcp.argtypes = [vp, vp, u64, vp, i32, vp, i32, u32]
     lib.dcx_check_sa.argtypes = [vp, vp, u64, vp, i32, u32, ctypes.POINTER(i32)]
     lib.dcx_shard_texts.argtypes = [vp, u32, u32, vp, vp]
+    lib.dcx_build_bwt.argtypes = [vp, vp, u64, vp, i32, vp, ctypes.POINTER(u64), u32]
     _lib = lib
     return lib
 
@@ -287,6 +288,26 @@ class Context:
         flags = DCX_DEVICE_PTRS | (DCX_LCP_PERMUTED if permuted else 0)
         _check(self.lib.dcx_build_lcp(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
                                       ctypes.c_void_p(lcp_ptr), lcp_width, flags))
+
+    def build_bwt(self, text, sa: np.ndarray):
+        """(BWT without the sentinel row, primary index) of a host text and its SA
+        (any integer array), as libsais64_bwt returns them."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        s = np.ascontiguousarray(np.asarray(sa).astype(np.uint64))
+        out = np.zeros(max(t.size, 1), np.uint8)
+        primary = ctypes.c_uint64()
+        _check(self.lib.dcx_build_bwt(self.h, t.ctypes.data if t.size else None, t.size,
+                                      s.ctypes.data if s.size else None, 64, out.ctypes.data,
+                                      ctypes.byref(primary), DCX_HOST_PTRS))
+        return out[: t.size], int(primary.value)
+
+    def build_bwt_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int, bwt_ptr: int) -> int:
+        """BWT of a device-resident text and SA into device memory; returns the primary index."""
+        primary = ctypes.c_uint64()
+        _check(self.lib.dcx_build_bwt(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
+                                      ctypes.c_void_p(bwt_ptr), ctypes.byref(primary), DCX_DEVICE_PTRS))
+        return int(primary.value)
 
     def check_sa_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int) -> bool:
         """GPU check of a device-resident SA against a device-resident text."""

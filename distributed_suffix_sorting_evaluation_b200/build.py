@@ -24,7 +24,8 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"
 HOST_CXX = "/usr/bin/g++"
 
 SOURCES = ["dcx.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "radix.cuh", "keys.cuh", "segsort.cuh", "small_sa.cuh", "level_kernels.cuh"]
+HEADERS = ["common.cuh", "radix.cuh", "keys.cuh", "segsort.cuh", "small_sa.cuh", "level_kernels.cuh", "lcp.cuh",
+           "bwt.cuh", "serve.cuh"]
 
 
 def _nvcc() -> str:

@@ -37,6 +37,7 @@
 #include "segsort.cuh"
 #include "small_sa.cuh"
 #include "lcp.cuh"
+#include "bwt.cuh"
 
 namespace dcx {
 
@@ -1639,6 +1640,48 @@ static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     DCX_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+// BWT (libsais64_bwt convention) of a text and its SA; returns the primary index.
+static uint64_t build_bwt(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, int sa_width, uint8_t* out,
+                          uint32_t flags) {
+    if (!(sa_width == 32 || sa_width == 40 || sa_width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (sa_width < 64 && n > (1ull << sa_width)) throw Error(DCX_ERR_ARG, "text too long for the SA width");
+    if (n == 0) return 0;
+    if (!text || !sa || !out) throw Error(DCX_ERR_ARG, "null pointer");
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    const size_t wb = sa_width / 8;
+    if (dev && sa_width != 40 && ((uintptr_t)sa % wb) != 0) throw Error(DCX_ERR_ARG, "SA not aligned to its width");
+    DBuf<uint8_t> t, sa_in, stage;
+    const uint8_t* dtext = text;
+    const void* dsa = sa;
+    uint8_t* dout = out;
+    if (!dev) {
+        t = DBuf<uint8_t>(&c, n, true);
+        sa_in = DBuf<uint8_t>(&c, n * wb, true);
+        stage = DBuf<uint8_t>(&c, n, true);
+        DCX_CUDA(cudaMemcpyAsync(t.get(), text, n, cudaMemcpyHostToDevice, c.stream));
+        DCX_CUDA(cudaMemcpyAsync(sa_in.get(), sa, n * wb, cudaMemcpyHostToDevice, c.stream));
+        dtext = t.get();
+        dsa = sa_in.get();
+        dout = stage.get();
+    }
+    DBuf<BwtScan> st(&c, 1);
+    unsigned long long* stw = reinterpret_cast<unsigned long long*>(st.get());  // first_zero, zeros, out_of_range
+    DCX_CUDA(cudaMemsetAsync(stw, 0xff, sizeof(unsigned long long), c.stream));
+    DCX_CUDA(cudaMemsetAsync(stw + 1, 0, 2 * sizeof(unsigned long long), c.stream));
+    k_bwt_primary<<<grid_for(n, 256), 256, 0, c.stream>>>(dsa, sa_width, n, st.get());
+    DCX_CHECK_LAUNCH();
+    const BwtScan h = d2h_scalar(c, st.get());
+    if (h.out_of_range || h.zeros != 1)
+        throw Error(DCX_ERR_ARG, "not a suffix array of the text (an entry >= n, or not exactly one 0)");
+    const uint64_t p = h.first_zero + 1;
+    k_bwt_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(dtext, n, dsa, sa_width, p, dout);
+    DCX_CHECK_LAUNCH();
+    c.launched(2);
+    if (!dev) DCX_CUDA(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    return p;
+}
+
 }  // namespace dcx
 
 #include "serve.cuh"
@@ -1858,6 +1901,16 @@ int dcx_build_lcp(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, i
         std::lock_guard<std::mutex> lk(x->c.build_mu);
         DCX_CUDA(cudaSetDevice(x->c.device));
         dcx::build_lcp(x->c, text, n, sa, sa_width, lcp_out, lcp_width, flags);
+    });
+}
+
+int dcx_build_bwt(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, int sa_width, uint8_t* bwt_out,
+                  uint64_t* primary_index, uint32_t flags) {
+    if (!x || !primary_index) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        *primary_index = dcx::build_bwt(x->c, text, n, sa, sa_width, bwt_out, flags);
     });
 }
 

@@ -124,6 +124,18 @@ int dcx_check_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, 
 int dcx_build_lcp(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
                   void* lcp_out, int lcp_width, uint32_t flags);
 
+/* ---- BWT ------------------------------------------------------------------- */
+/* Burrows-Wheeler transform of a text from its SA, in the convention of
+ * libsais64_bwt (libsais/include/libsais64.h:125-135): bwt_out[0..n) is the last
+ * column of the sorted rotations of T$ without the sentinel's row
+ * (bwt_out[0] = T[n-1], then T[SA[k]-1] for every SA[k] != 0 in SA order) and
+ * *primary_index = 1 + the k with SA[k] = 0, where that row would stand (0 for
+ * n = 0).  No counterpart in lightweight_dcx.  DCX_ERR_ARG when an SA entry is
+ * >= n or the SA has not exactly one 0 (a permutation is not checked:
+ * dcx_check_sa does that).  Host or device pointers as for dcx_build_sa. */
+int dcx_build_bwt(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
+                  uint8_t* bwt_out, uint64_t* primary_index, uint32_t flags);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
  * caller can time builds with events recorded on it. */
 int dcx_get_stream(dcx_ctx* ctx, void** stream_out);

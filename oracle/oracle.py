@@ -103,6 +103,8 @@ def _load_sais():
         lib.libsais64_plcp.restype = ctypes.c_int64
         lib.libsais64_lcp.argtypes = [_i64p, _i64p, _i64p, ctypes.c_int64]
         lib.libsais64_lcp.restype = ctypes.c_int64
+        lib.libsais64_bwt.argtypes = [_u8p, _u8p, _i64p, ctypes.c_int64, ctypes.c_int64, _i64p]
+        lib.libsais64_bwt.restype = ctypes.c_int64
         _sais = lib
     return _sais
 
@@ -214,6 +216,35 @@ def libsais_lcp(text: np.ndarray, sa: np.ndarray | None = None):
     if lib.libsais64_lcp(_ptr(plcp, _i64p), _ptr(s, _i64p), _ptr(lcp, _i64p), n) != 0:
         raise RuntimeError("libsais64_lcp failed")
     return plcp, lcp
+
+
+def libsais_bwt(text: np.ndarray):
+    """(U, primary index) of ``text`` by libsais64_bwt
+    (libsais/include/libsais64.h:125-135): U is the BWT without the sentinel
+    row, the primary index is where that row would stand."""
+    lib = _load_sais()
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    n = t.size
+    u = np.zeros(max(n, 1), np.uint8)
+    a = np.zeros(max(n, 1), np.int64)
+    p = lib.libsais64_bwt(_ptr(t if n else u, _u8p), _ptr(u, _u8p), _ptr(a, _i64p), n, 0, None)
+    if p < 0:
+        raise RuntimeError(f"libsais64_bwt failed: {p}")
+    return u[:n].copy(), int(p)
+
+
+def bwt_from_sa(text: np.ndarray, sa: np.ndarray):
+    """The same (U, primary index) restated from a suffix array: U[0] = T[n-1],
+    then T[SA[k]-1] for every SA[k] != 0 in SA order; primary = 1 + the k with
+    SA[k] = 0 (0 for the empty text)."""
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    n = t.size
+    if n == 0:
+        return np.zeros(0, np.uint8), 0
+    s = np.asarray(sa, dtype=np.int64)
+    z = int(np.flatnonzero(s == 0)[0])
+    rest = s[s != 0]
+    return np.concatenate([t[n - 1:], t[rest - 1]]).astype(np.uint8), z + 1
 
 
 def slow_sa(text: np.ndarray) -> np.ndarray:
