@@ -52,6 +52,7 @@ EXPORTED = (
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
     "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
+    "dcx_build_gsa",
 )
 
 # serving request states (dcx_serve_poll)
@@ -133,6 +134,7 @@ def load_library(path: str | None = None):
     lib.dcx_check_sa.argtypes = [vp, vp, u64, vp, i32, u32, ctypes.POINTER(i32)]
     lib.dcx_shard_texts.argtypes = [vp, u32, u32, vp, vp]
     lib.dcx_build_bwt.argtypes = [vp, vp, u64, vp, i32, vp, ctypes.POINTER(u64), u32]
+    lib.dcx_build_gsa.argtypes = [vp, vp, u64, i32, i32, vp, u32]
     _lib = lib
     return lib
 
@@ -288,6 +290,20 @@ class Context:
         flags = DCX_DEVICE_PTRS | (DCX_LCP_PERMUTED if permuted else 0)
         _check(self.lib.dcx_build_lcp(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
                                       ctypes.c_void_p(lcp_ptr), lcp_width, flags))
+
+    def build_gsa(self, text, dc: int = 39, sa_width: int = 64) -> np.ndarray:
+        """Generalized SA (uint64) of a string set given as a host byte array:
+        each string followed by a 0 byte, as libsais64_gsa takes it."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        raw = np.zeros(max(t.size, 1) * sa_dtype_bytes(sa_width), np.uint8)
+        _check(self.lib.dcx_build_gsa(self.h, t.ctypes.data if t.size else None, t.size, dc, sa_width,
+                                      raw.ctypes.data, DCX_HOST_PTRS))
+        return unpack_sa(raw, sa_width, t.size)
+
+    def build_gsa_device(self, text_ptr: int, n: int, sa_ptr: int, dc: int = 39, sa_width: int = 32):
+        _check(self.lib.dcx_build_gsa(self.h, ctypes.c_void_p(text_ptr), n, dc, sa_width, ctypes.c_void_p(sa_ptr),
+                                      DCX_DEVICE_PTRS))
 
     def build_bwt(self, text, sa: np.ndarray):
         """(BWT without the sentinel row, primary index) of a host text and its SA

@@ -38,6 +38,7 @@
 #include "small_sa.cuh"
 #include "lcp.cuh"
 #include "bwt.cuh"
+#include "gsa.cuh"
 
 namespace dcx {
 
@@ -1682,6 +1683,100 @@ static uint64_t build_bwt(Ctx& c, const uint8_t* text, uint64_t n, const void* s
     return p;
 }
 
+// Generalized SA of a string set (libsais64_gsa convention) from the plain SA:
+// runs of plain-SA neighbours that agree through their separators re-sorted by
+// position.
+static void build_gsa(Ctx& c, const uint8_t* text, uint64_t n, int X, int width, void* out, uint32_t flags) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    get_dc(c, (uint32_t)X);
+    if (n == 0) return;
+    if (!text || !out) throw Error(DCX_ERR_ARG, "null pointer");
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    const size_t wb = width / 8;
+    if (dev && width != 40 && ((uintptr_t)out % wb) != 0) throw Error(DCX_ERR_ARG, "SA not aligned to its width");
+    // the set, zero-padded: the LCP word loads read up to 15 bytes past its end
+    DBuf<uint8_t> t(&c, n + 16);
+    DCX_CUDA(cudaMemsetAsync(t.get() + n, 0, 16, c.stream));
+    DCX_CUDA(cudaMemcpyAsync(t.get(), text, n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+    {
+        DBuf<unsigned long long> bad(&c, 1);
+        DCX_CUDA(cudaMemsetAsync(bad.get(), 0, 8, c.stream));
+        k_gsa_check<<<grid_for(n, 256), 256, 0, c.stream>>>(t.get(), n, bad.get());
+        DCX_CHECK_LAUNCH();
+        if (d2h_scalar(c, bad.get()))
+            throw Error(DCX_ERR_ARG, "not a string set: the last byte must be 0 and no string may be empty");
+    }
+    if (n == 1) {  // the set "\0"
+        if (dev) DCX_CUDA(cudaMemsetAsync(out, 0, wb, c.stream));
+        else memset(out, 0, wb);
+        DCX_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    // plain SA of the whole set
+    DBuf<uint32_t> sa32(&c, n);
+    build_one(c, t.get(), n, X, 32, sa32.get(), DCX_DEVICE_PTRS | (flags & DCX_NO_PACKING), false);
+    // separators, capped PLCP, run heads
+    DBuf<uint8_t> head(&c, n);
+    {
+        DBuf<uint32_t> zb(&c, n), sep(&c, n / 2 + 1);  // no empty string: at most n/2 separators
+        device_scan<uint32_t>(c, OpSeparators{t.get(), zb.get(), sep.get()}, n);
+        DBuf<uint32_t> phi(&c, n), plcp(&c, n);
+        k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, phi.get());
+        k_plcp_to_separator<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(
+            t.get(), n, phi.get(), zb.get(), sep.get(), plcp.get());
+        DCX_CHECK_LAUNCH();
+        phi.reset();
+        k_gsa_heads<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, plcp.get(), zb.get(), sep.get(),
+                                                            head.get());
+        DCX_CHECK_LAUNCH();
+        c.launched(4);
+    }
+    // runs re-sorted by (run number, position)
+    {
+        DBuf<uint32_t> slot(&c, n), grp(&c, n), tpos(&c, n);
+        OpTied op{head.get(), n, sa32.get(), nullptr, slot.get(), grp.get(), tpos.get(), nullptr};
+        const uint64_t cnt = device_scan<uint64_t>(c, op, n) >> 32;
+        if (cnt) {
+            DBuf<uint32_t> k1[2], vals[2];
+            SortSpace s;
+            s.k[0][0] = tpos.get();
+            s.k[0][1] = grp.get();
+            for (int w = 0; w < 2; w++) {
+                k1[w] = DBuf<uint32_t>(&c, cnt);
+                s.k[1][w] = k1[w].get();
+                vals[w] = DBuf<uint32_t>(&c, cnt);
+                s.v[w] = vals[w].get();
+            }
+            DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+            SortPassArgs ha{};
+            ha.keys_in[0] = s.k[0][0];
+            ha.keys_in[1] = s.k[0][1];
+            ha.kw = 2;
+            ha.n = cnt;
+            k_digit_hist<<<grid_for(cnt, 256, 148 * 4), 256, 8 * RADIX * 4, c.stream>>>(ha, c.d_hist);
+            DCX_CHECK_LAUNCH();
+            const int f = radix_sort(c, 2, cnt, s);
+            k_gsa_scatter<<<grid_for(cnt, 256), 256, 0, c.stream>>>(cnt, slot.get(), s.k[f][0], sa32.get());
+            DCX_CHECK_LAUNCH();
+            c.launched(2);
+        }
+    }
+    head.reset();
+    DBuf<uint8_t> stage;
+    void* dout = out;
+    if (!dev) {
+        stage = DBuf<uint8_t>(&c, n * wb, true);
+        dout = stage.get();
+    }
+    k_store_sa<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, dout, width);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    if (!dev) DCX_CUDA(cudaMemcpyAsync(out, dout, n * wb, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_error(c);
+}
+
 }  // namespace dcx
 
 #include "serve.cuh"
@@ -1901,6 +1996,15 @@ int dcx_build_lcp(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, i
         std::lock_guard<std::mutex> lk(x->c.build_mu);
         DCX_CUDA(cudaSetDevice(x->c.device));
         dcx::build_lcp(x->c, text, n, sa, sa_width, lcp_out, lcp_width, flags);
+    });
+}
+
+int dcx_build_gsa(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, void* out, uint32_t flags) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::build_gsa(x->c, text, n, dc, w, out, flags);
     });
 }
 

@@ -124,6 +124,19 @@ int dcx_check_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, 
 int dcx_build_lcp(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
                   void* lcp_out, int lcp_width, uint32_t flags);
 
+/* ---- generalized SA ----------------------------------------------------------- */
+/* Generalized suffix array of a string set, in the convention of
+ * libsais64_gsa (libsais/include/libsais64.h:63-72): text holds the strings,
+ * each followed by a 0 byte (text[n-1] = 0; no empty string, except that the
+ * set may be the single byte 0), and sa_out receives all n suffixes ordered as
+ * if every separator were its own symbol below every character, separators in
+ * string order.  (The reference tree's other generalized-SA construction,
+ * psac's prefix doubling over a distributed string set,
+ * psac/include/suffix_array.hpp:283-380, needs MPI.)  `dc` and `sa_width` as for dcx_build_sa;
+ * DCX_ERR_ARG for a set libsais64_gsa refuses.  Host or device pointers. */
+int dcx_build_gsa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_width, void* sa_out,
+                  uint32_t flags);
+
 /* ---- BWT ------------------------------------------------------------------- */
 /* Burrows-Wheeler transform of a text from its SA, in the convention of
  * libsais64_bwt (libsais/include/libsais64.h:125-135): bwt_out[0..n) is the last

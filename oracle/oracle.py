@@ -105,6 +105,8 @@ def _load_sais():
         lib.libsais64_lcp.restype = ctypes.c_int64
         lib.libsais64_bwt.argtypes = [_u8p, _u8p, _i64p, ctypes.c_int64, ctypes.c_int64, _i64p]
         lib.libsais64_bwt.restype = ctypes.c_int64
+        lib.libsais64_gsa.argtypes = [_u8p, _i64p, ctypes.c_int64, ctypes.c_int64, _i64p]
+        lib.libsais64_gsa.restype = ctypes.c_int64
         _sais = lib
     return _sais
 
@@ -231,6 +233,37 @@ def libsais_bwt(text: np.ndarray):
     if p < 0:
         raise RuntimeError(f"libsais64_bwt failed: {p}")
     return u[:n].copy(), int(p)
+
+
+def libsais_gsa(text: np.ndarray) -> np.ndarray:
+    """Generalized SA of a string set (each string followed by a 0 byte) by
+    libsais64_gsa (libsais/include/libsais64.h:63-72)."""
+    lib = _load_sais()
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    n = t.size
+    sa = np.zeros(max(n, 1), np.int64)
+    rc = lib.libsais64_gsa(_ptr(t if n else np.zeros(1, np.uint8), _u8p), _ptr(sa, _i64p), n, 0, None)
+    if rc != 0:
+        raise RuntimeError(f"libsais64_gsa refused the set: {rc}")
+    return sa[:n].copy()
+
+
+def gsa_from_sa(text: np.ndarray) -> np.ndarray:
+    """The same order restated from the plain SA of the set: runs of plain-SA
+    neighbours whose LCP reaches through the suffix's separator, each sorted by
+    position (the construction the GPU follows)."""
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    n = t.size
+    if n <= 1:
+        return np.zeros(n, np.int64)
+    sa = libsais(t).astype(np.int64)
+    _, lcp = libsais_lcp(t, sa)
+    zpos = np.flatnonzero(t == 0)
+    to_sep = zpos[np.searchsorted(zpos, np.arange(n))] - np.arange(n) + 1
+    joins = np.zeros(n, bool)
+    joins[1:] = lcp[1:] >= to_sep[sa[1:]]
+    run = np.cumsum(~joins)  # run number of each plain-SA entry
+    return sa[np.lexsort((sa, run))]
 
 
 def bwt_from_sa(text: np.ndarray, sa: np.ndarray):

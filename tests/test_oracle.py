@@ -132,3 +132,34 @@ def test_libsais_bwt_known_answer_and_restatement(oracle):
         u, p = oracle.libsais_bwt(t)
         u2, p2 = oracle.bwt_from_sa(t, oracle.libsais(t))
         assert p == p2 and np.array_equal(u, u2)
+
+
+def _string_set(rng, k, sigma, base):
+    parts = []
+    for _ in range(k):
+        m = rng.integers(0, 3)
+        if m == 0:
+            s = rng.integers(1, 1 + sigma, rng.integers(1, 40))
+        elif m == 1:
+            s = base[rng.integers(0, base.size):]
+        else:
+            s = base
+        parts.append(np.concatenate([s, [0]]))
+    return np.concatenate(parts).astype(np.uint8)
+
+
+def test_libsais_gsa_known_answer_and_restatement(oracle):
+    """libsais64_gsa orders the suffixes of a 0-separated string set as if each
+    separator were its own symbol, smallest, in string order; the plain-SA
+    regrouping the GPU follows gives the same array."""
+    t = np.frombuffer(b"ab\0ab\0", np.uint8)
+    assert oracle.libsais_gsa(t).tolist() == [2, 5, 0, 3, 1, 4]
+    t = np.frombuffer(b"banana\0ana\0", np.uint8)
+    assert oracle.libsais_gsa(t).tolist() == [6, 10, 5, 9, 3, 7, 1, 0, 4, 8, 2]
+    with pytest.raises(RuntimeError):
+        oracle.libsais_gsa(np.frombuffer(b"a\0\0", np.uint8))  # empty string
+    rng = np.random.default_rng(2)
+    for _ in range(200):
+        base = rng.integers(1, 4, rng.integers(1, 50))
+        t = _string_set(rng, int(rng.integers(1, 30)), 3, base)
+        assert np.array_equal(oracle.gsa_from_sa(t), oracle.libsais_gsa(t))
