@@ -42,6 +42,7 @@ DCX_NO_PACKING = 2
 DCX_NO_REMAP = 4
 DCX_SERVE_BORROW = 8
 DCX_LCP_PERMUTED = 16
+DCX_LCP_GSA = 32
 
 SUPPORTED_DC = (3, 7, 13, 21, 31, 39, 57, 73, 91, 95, 133)
 
@@ -273,13 +274,14 @@ class Context:
                                      ctypes.byref(ok)))
         return bool(ok.value)
 
-    def build_lcp(self, text, sa: np.ndarray, permuted: bool = False) -> np.ndarray:
-        """LCP array (or PLCP) of a host text and its SA (any integer array)."""
+    def build_lcp(self, text, sa: np.ndarray, permuted: bool = False, gsa: bool = False) -> np.ndarray:
+        """LCP array (or PLCP) of a host text and its SA (any integer array); with
+        gsa=True, of a 0-separated string set and its generalized SA."""
         t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
                                  else np.asarray(text, dtype=np.uint8))
         s = np.ascontiguousarray(np.asarray(sa).astype(np.uint64))
         out = np.zeros(max(t.size, 1), np.uint64)
-        flags = DCX_HOST_PTRS | (DCX_LCP_PERMUTED if permuted else 0)
+        flags = DCX_HOST_PTRS | (DCX_LCP_PERMUTED if permuted else 0) | (DCX_LCP_GSA if gsa else 0)
         if t.size:
             _check(self.lib.dcx_build_lcp(self.h, t.ctypes.data, t.size, s.ctypes.data, 64, out.ctypes.data, 64,
                                           flags))

@@ -1624,7 +1624,17 @@ static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, phi.get());
     DCX_CHECK_LAUNCH();
     sa_in.reset();
-    k_plcp<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(t.get(), n, phi.get(), plcp.get());
+    if (flags & DCX_LCP_GSA) {
+        // a generalized SA: separators (0 bytes) are distinct symbols, no match runs through one
+        if (d2h_scalar(c, t.get() + n - 1) != 0) throw Error(DCX_ERR_ARG, "a string set ends with a 0 byte");
+        DBuf<uint32_t> zb(&c, n), sep(&c, n);
+        device_scan<uint32_t>(c, OpSeparators{t.get(), zb.get(), sep.get()}, n);
+        k_plcp_to_separator<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(
+            t.get(), n, phi.get(), zb.get(), sep.get(), plcp.get(), 0);
+        c.launched();
+    } else {
+        k_plcp<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(t.get(), n, phi.get(), plcp.get());
+    }
     DCX_CHECK_LAUNCH();
     phi.reset();
     DBuf<uint8_t> stage;
@@ -1724,7 +1734,7 @@ static void build_gsa(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         DBuf<uint32_t> phi(&c, n), plcp(&c, n);
         k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, phi.get());
         k_plcp_to_separator<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(
-            t.get(), n, phi.get(), zb.get(), sep.get(), plcp.get());
+            t.get(), n, phi.get(), zb.get(), sep.get(), plcp.get(), 1);
         DCX_CHECK_LAUNCH();
         phi.reset();
         k_gsa_heads<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, plcp.get(), zb.get(), sep.get(),

@@ -52,11 +52,14 @@ __device__ __forceinline__ uint64_t to_separator(const uint32_t* __restrict__ ze
     return (uint64_t)sep_pos[zeros_before[i]] - i + 1;  // chars of suffix i through its separator
 }
 
-// PLCP[i] = min(lcp(i, Phi[i]), to_separator(i)) for a text padded with at
-// least 16 readable bytes past its end (16-byte aligned base).
+// PLCP[i] = min(lcp(i, Phi[i]), to_separator(i) - 1 + through) for a text
+// padded with at least 16 readable bytes past its end (16-byte aligned base):
+// through = 1 counts the separator as a match (the runs of the GSA
+// construction), through = 0 stops before it (the LCP of a GSA, where
+// separators are distinct symbols and never match).
 __global__ void k_plcp_to_separator(const uint8_t* __restrict__ text, uint64_t n, const uint32_t* __restrict__ phi,
                                     const uint32_t* __restrict__ zeros_before, const uint32_t* __restrict__ sep_pos,
-                                    uint32_t* __restrict__ plcp) {
+                                    uint32_t* __restrict__ plcp, uint32_t through) {
     const uint64_t* tw = reinterpret_cast<const uint64_t*>(text);
     const uint64_t runs = (n + LCP_RUN - 1) / LCP_RUN;
     for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < runs; r += (uint64_t)gridDim.x * blockDim.x) {
@@ -71,7 +74,7 @@ __global__ void k_plcp_to_separator(const uint8_t* __restrict__ text, uint64_t n
                 continue;
             }
             const uint64_t shorter = n - (i > j ? i : (uint64_t)j);
-            const uint64_t cap = to_separator(zeros_before, sep_pos, i);
+            const uint64_t cap = to_separator(zeros_before, sep_pos, i) - 1 + through;
             const uint64_t lim = cap < shorter ? cap : shorter;
             if (h > lim) h = lim;
             while (h < lim) {

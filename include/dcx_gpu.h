@@ -121,6 +121,11 @@ int dcx_check_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, 
  * lcp_width is 32 or 64.  No counterpart in lightweight_dcx, whose SA is the
  * usual input of this step.  Host or device pointers as for dcx_build_sa. */
 #define DCX_LCP_PERMUTED 16
+/* With DCX_LCP_GSA, sa is a generalized SA of a 0-separated string set
+ * (dcx_build_gsa) and every separator is its own symbol: no common prefix runs
+ * through one, as libsais64_plcp_gsa computes it (libsais/include/libsais64.h:
+ * 245-253).  DCX_ERR_ARG unless text[n-1] = 0. */
+#define DCX_LCP_GSA 32
 int dcx_build_lcp(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
                   void* lcp_out, int lcp_width, uint32_t flags);
 

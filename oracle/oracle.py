@@ -107,6 +107,8 @@ def _load_sais():
         lib.libsais64_bwt.restype = ctypes.c_int64
         lib.libsais64_gsa.argtypes = [_u8p, _i64p, ctypes.c_int64, ctypes.c_int64, _i64p]
         lib.libsais64_gsa.restype = ctypes.c_int64
+        lib.libsais64_plcp_gsa.argtypes = [_u8p, _i64p, _i64p, ctypes.c_int64]
+        lib.libsais64_plcp_gsa.restype = ctypes.c_int64
         _sais = lib
     return _sais
 
@@ -246,6 +248,24 @@ def libsais_gsa(text: np.ndarray) -> np.ndarray:
     if rc != 0:
         raise RuntimeError(f"libsais64_gsa refused the set: {rc}")
     return sa[:n].copy()
+
+
+def libsais_lcp_gsa(text: np.ndarray, gsa: np.ndarray | None = None):
+    """(PLCP, LCP) of a string set and its generalized SA by libsais64_plcp_gsa
+    / libsais64_lcp: separators are distinct symbols and never match."""
+    lib = _load_sais()
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    n = t.size
+    if n == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    g = libsais_gsa(t) if gsa is None else np.ascontiguousarray(gsa, dtype=np.int64)
+    plcp = np.zeros(n, np.int64)
+    lcp = np.zeros(n, np.int64)
+    if lib.libsais64_plcp_gsa(_ptr(t, _u8p), _ptr(g, _i64p), _ptr(plcp, _i64p), n) != 0:
+        raise RuntimeError("libsais64_plcp_gsa failed")
+    if lib.libsais64_lcp(_ptr(plcp, _i64p), _ptr(g, _i64p), _ptr(lcp, _i64p), n) != 0:
+        raise RuntimeError("libsais64_lcp failed")
+    return plcp, lcp
 
 
 def gsa_from_sa(text: np.ndarray) -> np.ndarray:

@@ -50,3 +50,55 @@ def reference_file(*parts):
 def random_text(n, sigma, seed, offset=65):
     rng = np.random.default_rng(seed)
     return rng.integers(offset, offset + sigma, n).astype(np.uint8)
+
+
+def psac_gsa_case(seq: str, reps: int):
+    """The string sets of the reference's generalized-SA tests
+    (psac/test/test_gsa.cpp:24-30, 145-178): `reps` strings, the j-th being
+    `seq` repeated j+1 times.  Returns (strings, expected GSA over the
+    concatenation without separators) with the expectation restated from
+    psac/test/test_gsa.cpp:32-50: for each offset i inside one copy of `seq`,
+    and each string j whose copy holds the next smallest suffix, the suffix of
+    string j at i, then that suffix's equal in every longer string, each one
+    copy of `seq` (k*len(seq) positions) further along."""
+    L = len(seq)
+    strings = [seq * (j + 1) for j in range(reps)]
+    expected = []
+    for i in range(L):
+        for j in range(reps):
+            pos = i + L * (j * (j + 1) // 2)  # offset i in string j
+            expected.append(pos)
+            for k in range(j + 2, reps + 1):
+                pos += k * L
+                expected.append(pos)
+    return strings, expected
+
+
+PSAC_GSA_CASES = [("ab", 3), ("abc", 3), ("a", 20), ("abc", 10), ("abcdef", 50)]
+
+
+def flat_positions(text: np.ndarray, gsa: np.ndarray) -> list:
+    """A generalized SA over a 0-separated set, without the separators and with
+    positions counted in the concatenation without separators (psac's layout)."""
+    g = np.asarray(gsa, dtype=np.int64)
+    sep_before = np.concatenate([[0], np.cumsum(text == 0)[:-1]])
+    keep = text[g] != 0
+    return (g[keep] - sep_before[g[keep]]).tolist()
+
+
+def set_bytes(strings) -> np.ndarray:
+    return np.frombuffer(b"".join(s.encode() + b"\0" for s in strings), np.uint8).copy()
+
+
+def psac_glcp_case(seq: str, reps: int) -> list:
+    """The LCP array psac's GSA tests expect beside psac_gsa_case's GSA
+    (psac/test/test_gsa.cpp:52-67), restated: for each offset i inside one copy
+    of `seq`, a 0 for the first suffix at i, then for j = 1 .. reps-1 the value
+    j*len(seq) - i once for each of the reps+1-j suffixes sharing it."""
+    L = len(seq)
+    out = []
+    for i in range(L):
+        out.append(0)
+        for j in range(1, reps):
+            out.extend([j * L - i] * (reps + 1 - j))
+    return out

@@ -61,3 +61,36 @@ def test_gsa_refuses_what_libsais_refuses(ctx):
         with pytest.raises(DcxError):
             ctx.build_gsa(np.frombuffer(bad, np.uint8))
     assert ctx.build_gsa(np.zeros(0, np.uint8)).size == 0
+
+
+def test_gsa_on_the_psac_test_sets(ctx):
+    """The string sets of the reference's psac GSA tests, checked against the
+    arrays those tests expect."""
+    from conftest import PSAC_GSA_CASES, flat_positions, psac_gsa_case, set_bytes
+    t = set_bytes(["abab", "baba"])
+    assert flat_positions(t, ctx.build_gsa(t)) == [7, 2, 5, 0, 3, 6, 1, 4]
+    for seq, reps in PSAC_GSA_CASES:
+        strings, expected = psac_gsa_case(seq, reps)
+        t = set_bytes(strings)
+        assert flat_positions(t, ctx.build_gsa(t)) == expected
+
+
+@pytest.mark.parametrize("idx", range(9))
+def test_gsa_lcp_matches_libsais(ctx, oracle, idx):
+    """LCP of a generalized SA (separators never match) against
+    libsais64_plcp_gsa + libsais64_lcp, from the GPU-built GSA."""
+    t = _cases()[idx]
+    g = ctx.build_gsa(t)
+    plcp, lcp = oracle.libsais_lcp_gsa(t, g.astype(np.int64))
+    assert np.array_equal(ctx.build_lcp(t, g, gsa=True), lcp.astype(np.uint64))
+    assert np.array_equal(ctx.build_lcp(t, g, permuted=True, gsa=True), plcp.astype(np.uint64))
+
+
+def test_gsa_lcp_on_the_psac_test_sets(ctx):
+    from conftest import PSAC_GSA_CASES, psac_gsa_case, psac_glcp_case, set_bytes
+    for seq, reps in PSAC_GSA_CASES:
+        strings, _ = psac_gsa_case(seq, reps)
+        t = set_bytes(strings)
+        g = ctx.build_gsa(t)
+        lcp = ctx.build_lcp(t, g, gsa=True)
+        assert lcp[t[g.astype(np.int64)] != 0].tolist() == psac_glcp_case(seq, reps)

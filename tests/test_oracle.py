@@ -163,3 +163,20 @@ def test_libsais_gsa_known_answer_and_restatement(oracle):
         base = rng.integers(1, 4, rng.integers(1, 50))
         t = _string_set(rng, int(rng.integers(1, 30)), 3, base)
         assert np.array_equal(oracle.gsa_from_sa(t), oracle.libsais_gsa(t))
+
+
+@pytest.mark.parametrize("seq,reps", [("ab", 3), ("abc", 3), ("a", 20), ("abc", 10), ("abcdef", 50)])
+def test_libsais_gsa_equals_psac_test_expectations(oracle, seq, reps):
+    """The generalized SA the GPU reproduces (libsais64_gsa's) is, without its
+    separator positions, the array the reference's psac GSA tests expect."""
+    from conftest import flat_positions, psac_gsa_case, set_bytes
+    strings, expected = psac_gsa_case(seq, reps)
+    t = set_bytes(strings)
+    assert flat_positions(t, oracle.libsais_gsa(t)) == expected
+    from conftest import psac_glcp_case
+    _, lcp = oracle.libsais_lcp_gsa(t)
+    assert lcp[t[oracle.libsais_gsa(t)] != 0].tolist() == psac_glcp_case(seq, reps)
+    t = set_bytes(["abab", "baba"])  # psac/test/test_gsa.cpp:71-101
+    g = oracle.libsais_gsa(t)
+    assert flat_positions(t, g) == [7, 2, 5, 0, 3, 6, 1, 4]
+    assert oracle.libsais_lcp_gsa(t, g)[1][t[g] != 0].tolist() == [0, 1, 2, 3, 0, 1, 2, 3]
