@@ -494,6 +494,16 @@ def run_batch(args, world, rank, local):
     d_sa = torch.empty(big + 16, dtype=torch.int32, device=dev)
     h_text = torch.empty(big + 16, dtype=torch.uint8, pin_memory=True)
     ctx = Context(local)
+    tuned = None
+    if args.batch_autotune:
+        # size-class DCs from a sample of the workload's own distribution (other
+        # seeds), tuned before the timed region
+        slens = W.batch_lengths(400, 1 << 10, 16 << 20, seed=11)
+        sample = [W.iid(int(m), b"ACGT", seed=2_000_000 + i) for i, m in enumerate(slens)]
+        bounds = [16 << 10, 256 << 10, 2 << 20, 16 << 20]
+        chosen, ms_tab = ctx.autotune_batch(sample, bounds, candidates=(3, 7, 13, 21, 39), repeats=2)
+        tuned = {"classes_max_len": bounds, "dc": chosen, "ms": ms_tab.round(3).tolist()}
+        del sample
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -580,7 +590,8 @@ def run_batch(args, world, rank, local):
             "data": "synthetic (seeded i.i.d. {A,C,G,T} texts, log-uniform lengths 1 KiB-16 MiB)",
             "config": {"workload": "cfg4_batch", "texts": int(all_lens.size), "text_bytes": int(all_lens.sum()),
                        "job_bytes": int(job_bytes), "rank0_texts": int(lens.size), "rank0_bytes": total,
-                       "chunk_mib": args.batch_chunk_mib, "dc": "auto per text", "sa_width": 32,
+                       "chunk_mib": args.batch_chunk_mib,
+                       "dc": tuned if tuned else "DC39 above the in-CTA base case (2048 chars)", "sa_width": 32,
                        "l2_flush": "each chunk's text and SAs are larger than L2",
                        "parallelism": split},
             "seconds": round(ms_total / 1000.0, 3),
@@ -855,6 +866,8 @@ def main():
                     help="context option (dcx_set_option) for the single-text workloads")
     ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
+    ap.add_argument("--batch-autotune", action="store_true",
+                    help="tune the DC per size class (dcx_autotune_batch) before the batched timing")
     ap.add_argument("--batch-split", default="lpt", choices=["lpt", "replicas"],
                     help="how the batched workload is split over ranks under torchrun")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")

@@ -53,7 +53,7 @@ EXPORTED = (
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
     "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
-    "dcx_build_gsa",
+    "dcx_build_gsa", "dcx_set_batch_dc_table", "dcx_get_batch_dc_table", "dcx_autotune_batch",
 )
 
 # serving request states (dcx_serve_poll)
@@ -136,6 +136,9 @@ def load_library(path: str | None = None):
     lib.dcx_shard_texts.argtypes = [vp, u32, u32, vp, vp]
     lib.dcx_build_bwt.argtypes = [vp, vp, u64, vp, i32, vp, ctypes.POINTER(u64), u32]
     lib.dcx_build_gsa.argtypes = [vp, vp, u64, i32, i32, vp, u32]
+    lib.dcx_set_batch_dc_table.argtypes = [vp, vp, vp, u32]
+    lib.dcx_get_batch_dc_table.argtypes = [vp, vp, vp, u32, ctypes.POINTER(u32)]
+    lib.dcx_autotune_batch.argtypes = [vp, vp, vp, u32, vp, u32, vp, u32, u32, vp, vp]
     _lib = lib
     return lib
 
@@ -292,6 +295,40 @@ class Context:
         flags = DCX_DEVICE_PTRS | (DCX_LCP_PERMUTED if permuted else 0)
         _check(self.lib.dcx_build_lcp(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
                                       ctypes.c_void_p(lcp_ptr), lcp_width, flags))
+
+    def set_batch_dc_table(self, table):
+        """[(longest text of the class, X), ...] ascending; [] restores DC39."""
+        ml = np.ascontiguousarray([int(a) for a, _ in table], dtype=np.uint64)
+        dc = np.ascontiguousarray([int(b) for _, b in table], dtype=np.int32)
+        _check(self.lib.dcx_set_batch_dc_table(self.h, ml.ctypes.data if ml.size else None,
+                                               dc.ctypes.data if dc.size else None, len(table)))
+
+    def batch_dc_table(self):
+        cnt = ctypes.c_uint32()
+        _check(self.lib.dcx_get_batch_dc_table(self.h, None, None, 0, ctypes.byref(cnt)))
+        ml = np.zeros(max(cnt.value, 1), np.uint64)
+        dc = np.zeros(max(cnt.value, 1), np.int32)
+        _check(self.lib.dcx_get_batch_dc_table(self.h, ml.ctypes.data, dc.ctypes.data, cnt.value, ctypes.byref(cnt)))
+        return [(int(ml[i]), int(dc[i])) for i in range(cnt.value)]
+
+    def autotune_batch(self, texts, class_max_len, candidates=(3, 7, 13, 21, 39), repeats: int = 3):
+        """Times each candidate DC on the sample texts of each size class and
+        installs the fastest per class; returns (chosen DC per class, median ms
+        [class][candidate])."""
+        ts = [np.ascontiguousarray(np.frombuffer(t, np.uint8) if isinstance(t, (bytes, bytearray))
+                                   else np.asarray(t, dtype=np.uint8)) for t in texts]
+        offs = np.zeros(len(ts) + 1, np.uint64)
+        offs[1:] = np.cumsum([t.size for t in ts], dtype=np.uint64)
+        cat = np.concatenate(ts) if ts else np.zeros(0, np.uint8)
+        cat = np.ascontiguousarray(cat if cat.size else np.zeros(1, np.uint8))
+        cm = np.ascontiguousarray(class_max_len, dtype=np.uint64)
+        cd = np.ascontiguousarray(candidates, dtype=np.int32)
+        chosen = np.zeros(cm.size, np.int32)
+        ms = np.zeros(cm.size * cd.size, np.float64)
+        _check(self.lib.dcx_autotune_batch(self.h, cat.ctypes.data, offs.ctypes.data, len(ts), cm.ctypes.data,
+                                           cm.size, cd.ctypes.data, cd.size, repeats, chosen.ctypes.data,
+                                           ms.ctypes.data))
+        return chosen.tolist(), ms.reshape(cm.size, cd.size)
 
     def build_gsa(self, text, dc: int = 39, sa_width: int = 64) -> np.ndarray:
         """Generalized SA (uint64) of a string set given as a host byte array:

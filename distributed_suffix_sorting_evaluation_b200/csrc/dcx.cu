@@ -204,6 +204,9 @@ struct Options {
     int trace = 0;
     uint32_t spin_limit = 1u << 24;
     uint64_t batch_round_cap = 0;  // max elements per batch round (0 = from the budget)
+    // DC per size class of batched builds with dc_or_auto = 0: (longest text of
+    // the class, X), ascending; longer texts and an empty table use DC39
+    std::vector<std::pair<uint64_t, uint32_t>> batch_dc;
     // serving
     uint32_t serve_lanes = 1;
     uint64_t serve_budget = 0;  // 0 = the context budget
@@ -1420,13 +1423,23 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
 // remap of a round is the union of its texts' alphabets, which keeps every
 // text's order (and therefore its SA) unchanged.
 // ---------------------------------------------------------------------------
+// X of a text of length len in a batched build with dc_or_auto = 0.
+static uint32_t batch_x_for(const Options& o, uint64_t len) {
+    for (const auto& e : o.batch_dc)
+        if (len <= e.first) return e.second;
+    return 39u;
+}
+
 static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, uint32_t K, int dc_or_auto, int width,
                         void* sa_out, uint32_t flags) {
     if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
     if (K == 0) return;
     if (!offsets || !texts || !sa_out) throw Error(DCX_ERR_ARG, "null pointer");
-    const uint32_t X = dc_or_auto == 0 ? 39u : (uint32_t)dc_or_auto;  // auto: DC39 for every DCX-sized text
+    const uint32_t X = dc_or_auto == 0 ? 39u : (uint32_t)dc_or_auto;  // auto: DC39 unless the size-class table says
     get_dc(c, X);
+    const bool by_class = dc_or_auto == 0 && !c.opt.batch_dc.empty();
+    if (by_class)
+        for (const auto& e : c.opt.batch_dc) get_dc(c, e.second);
     const bool dev = flags & DCX_DEVICE_PTRS;
     const bool packing = !(flags & DCX_NO_PACKING);
     const size_t wb = width / 8;
@@ -1520,7 +1533,7 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
             rstage = DBuf<uint8_t>(&c, std::max<uint64_t>(in_bytes, 1) * wb + 16, true);
             rout = rstage.get();
         }
-        auto run_group = [&](const Segs& g, const std::vector<uint32_t>& ids) {
+        auto run_group = [&](const Segs& g, const std::vector<uint32_t>& ids, uint32_t Xg) {
             if (ids.empty()) return;
             const uint32_t Kg = g.K();
             std::vector<uint64_t> goff(Kg + 1, 0), gsrc(Kg), cbase(Kg + 1, 0);
@@ -1541,18 +1554,31 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
                 k_spread_texts<uint32_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), d_cbase.get(),
                                                                        Kg, chunks, buf.get(), d_map.get(), true);
                 DCX_CHECK_LAUNCH();
-                level<uint32_t>(c, buf.get(), gd, sigma, X, 0, packing, rout, width);
+                level<uint32_t>(c, buf.get(), gd, sigma, Xg, 0, packing, rout, width);
             } else {
                 DBuf<uint8_t> buf(&c, Ng + 16);
                 k_spread_texts<uint8_t><<<blocks, 256, 0, c.stream>>>(dsrc, d_gsrc.get(), d_goff.get(), d_cbase.get(),
                                                                       Kg, chunks, buf.get(), d_map.get(), false);
                 DCX_CHECK_LAUNCH();
-                level<uint8_t>(c, buf.get(), gd, sigma, X, 0, packing, rout, width);
+                level<uint8_t>(c, buf.get(), gd, sigma, Xg, 0, packing, rout, width);
             }
             c.launched();
         };
-        run_group(small, small_ids);
-        run_group(big, big_ids);
+        run_group(small, small_ids, X);
+        if (by_class) {
+            // one group per X of the size-class table, each a level of its own
+            std::map<uint32_t, std::pair<Segs, std::vector<uint32_t>>> by_x;
+            for (uint32_t id : big_ids) {
+                const uint64_t len = in_off[id + 1] - in_off[id];
+                auto& e = by_x[batch_x_for(c.opt, len)];
+                if (e.first.start.empty()) e.first.start = {0};
+                e.first.start.push_back(e.first.start.back() + len + 1);
+                e.second.push_back(id);
+            }
+            for (const auto& kv : by_x) run_group(kv.second.first, kv.second.second, kv.first);
+        } else {
+            run_group(big, big_ids, X);
+        }
         if (!dev && in_bytes)
             DCX_CUDA(cudaMemcpyAsync((uint8_t*)sa_out + (offsets[s0] - base0) * wb, rout, in_bytes * wb,
                                      cudaMemcpyDeviceToHost, c.stream));
@@ -1567,6 +1593,68 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
     c.st.peak_bytes = c.peak;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+// Autotuner of the size-class table: the texts of a host sample batch in each
+// class (length in (class_max[i-1], class_max[i]]) are built as one batch with
+// each candidate X (device-resident, one warm-up, median device time of
+// `repeats` runs), and the fastest X per class becomes the context's table.
+// Classes without sample texts keep DC39 (chosen[i] = 0).
+static void autotune_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, uint32_t K,
+                           const uint64_t* class_max, uint32_t ncls, const int* cand, uint32_t ncand,
+                           uint32_t repeats, int* chosen, double* ms_out) {
+    if (!texts || !offsets || !class_max || !cand || !chosen || K == 0 || ncls == 0 || ncand == 0)
+        throw Error(DCX_ERR_ARG, "null pointer or empty sample / classes / candidates");
+    for (uint32_t i = 1; i < ncls; i++)
+        if (class_max[i] <= class_max[i - 1]) throw Error(DCX_ERR_ARG, "class bounds must ascend");
+    for (uint32_t j = 0; j < ncand; j++) {
+        if (cand[j] <= 0) throw Error(DCX_ERR_ARG, "unsupported difference cover");
+        get_dc(c, (uint32_t)cand[j]);
+    }
+    for (uint32_t s = 0; s < K; s++)
+        if (offsets[s + 1] < offsets[s]) throw Error(DCX_ERR_ARG, "offsets must be non-decreasing");
+    repeats = std::max<uint32_t>(repeats, 1);
+    std::vector<std::pair<uint64_t, uint32_t>> table;
+    for (uint32_t i = 0; i < ncls; i++) {
+        const uint64_t lo = i ? class_max[i - 1] : 0, hi = class_max[i];
+        std::vector<uint64_t> offs = {0};
+        std::vector<uint8_t> cat;
+        for (uint32_t s = 0; s < K; s++) {
+            const uint64_t len = offsets[s + 1] - offsets[s];
+            if (len <= lo || len > hi) continue;
+            const uint8_t* src = texts + (offsets[s] - offsets[0]);
+            cat.insert(cat.end(), src, src + len);
+            offs.push_back(offs.back() + len);
+        }
+        chosen[i] = 0;
+        if (offs.size() == 1) {
+            if (ms_out)
+                for (uint32_t j = 0; j < ncand; j++) ms_out[(size_t)i * ncand + j] = -1.0;
+            continue;
+        }
+        const uint32_t Kc = (uint32_t)(offs.size() - 1);
+        const uint64_t bytes = offs.back();
+        DBuf<uint8_t> d_text(&c, bytes + 16);
+        DBuf<uint32_t> d_sa(&c, std::max<uint64_t>(bytes, 1));
+        DCX_CUDA(cudaMemcpyAsync(d_text.get(), cat.data(), bytes, cudaMemcpyHostToDevice, c.stream));
+        double best = 0;
+        for (uint32_t j = 0; j < ncand; j++) {
+            std::vector<double> t;
+            for (uint32_t r = 0; r <= repeats; r++) {
+                build_batch(c, d_text.get(), offs.data(), Kc, cand[j], 32, d_sa.get(), DCX_DEVICE_PTRS);
+                if (r) t.push_back(c.st.ms_total);
+            }
+            std::sort(t.begin(), t.end());
+            const double med = t[t.size() / 2];
+            if (ms_out) ms_out[(size_t)i * ncand + j] = med;
+            if (chosen[i] == 0 || med < best) {
+                best = med;
+                chosen[i] = cand[j];
+            }
+        }
+        table.push_back({hi, (uint32_t)chosen[i]});
+    }
+    c.opt.batch_dc = table;
 }
 
 // Checks that sa (n entries of `width` bits) is the suffix array of text.
@@ -2071,6 +2159,46 @@ int dcx_build_sa_batch(dcx_ctx* x, const uint8_t* texts, const uint64_t* offsets
         dcx::build_batch(x->c, texts, offsets, num_texts, dc_or_auto, sa_width, sa_out, flags);
     });
 }
+int dcx_set_batch_dc_table(dcx_ctx* x, const uint64_t* max_len, const int* dc, uint32_t count) {
+    if (!x || (count && (!max_len || !dc))) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        std::vector<std::pair<uint64_t, uint32_t>> t;
+        for (uint32_t i = 0; i < count; i++) {
+            if (i && max_len[i] <= max_len[i - 1]) throw dcx::Error(DCX_ERR_ARG, "class bounds must ascend");
+            if (dc[i] <= 0) throw dcx::Error(DCX_ERR_ARG, "unsupported difference cover");
+            dcx::get_dc(x->c, (uint32_t)dc[i]);
+            t.push_back({max_len[i], (uint32_t)dc[i]});
+        }
+        x->c.opt.batch_dc = t;
+    });
+}
+
+int dcx_get_batch_dc_table(dcx_ctx* x, uint64_t* max_len, int* dc, uint32_t capacity, uint32_t* count) {
+    if (!x || !count) return DCX_ERR_ARG;
+    std::lock_guard<std::mutex> lk(x->c.build_mu);
+    const auto& t = x->c.opt.batch_dc;
+    *count = (uint32_t)t.size();
+    for (uint32_t i = 0; i < capacity && i < t.size(); i++) {
+        if (max_len) max_len[i] = t[i].first;
+        if (dc) dc[i] = (int)t[i].second;
+    }
+    return DCX_OK;
+}
+
+int dcx_autotune_batch(dcx_ctx* x, const uint8_t* texts, const uint64_t* offsets, uint32_t num_texts,
+                       const uint64_t* class_max_len, uint32_t num_classes, const int* candidates,
+                       uint32_t num_candidates, uint32_t repeats, int* chosen_dc, double* ms_out) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::autotune_batch(x->c, texts, offsets, num_texts, class_max_len, num_classes, candidates, num_candidates,
+                            repeats, chosen_dc, ms_out);
+    });
+}
+
 static dcx::Server& server_of(dcx_ctx* x) {
     std::lock_guard<std::mutex> lk(x->serve_mu);
     if (!x->server) {

@@ -170,11 +170,34 @@ int dcx_get_trace(dcx_ctx* ctx, uint64_t* m_out, uint32_t* names, uint8_t* uniqu
 /* Builds one SA per text.  texts is the concatenation, offsets[num_texts+1] the
  * text boundaries (offsets[0] = 0).  sa_out receives, per text, its SA with
  * text-local indices, concatenated in the same layout as texts.  dc_or_auto = 0
- * lets the autotuner pick X per size class.  Every text must be < 2^32 - 1 bytes;
+ * takes X per size class from the table below (dcx_set_batch_dc_table /
+ * dcx_autotune_batch; DC39 without one).  Every text must be < 2^32 - 1 bytes;
  * the concatenation may be larger than one build fits: it is split into rounds. */
 int dcx_build_sa_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offsets,
                        uint32_t num_texts, int dc_or_auto, int sa_width, void* sa_out,
                        uint32_t flags);
+
+/* Size-class table of dcx_build_sa_batch with dc_or_auto = 0: a text longer
+ * than the in-CTA base case uses dc[i] for the first i with length <=
+ * max_len[i] (max_len ascending), DC39 when no class holds it; count = 0
+ * restores DC39 for all.  The texts of each X are built as one group.  Any X
+ * gives the same SAs; the table only changes the speed.  Serving lanes take the
+ * table in force at the first dcx_serve_submit. */
+int dcx_set_batch_dc_table(dcx_ctx* ctx, const uint64_t* max_len, const int* dc, uint32_t count);
+/* Copies up to `capacity` entries of the table; *count = its length. */
+int dcx_get_batch_dc_table(dcx_ctx* ctx, uint64_t* max_len, int* dc, uint32_t capacity, uint32_t* count);
+/* Autotuner of that table.  The texts of a sample batch in HOST memory (layout
+ * of dcx_build_sa_batch) are split into size classes (length in
+ * (class_max_len[i-1], class_max_len[i]]); each class is built as one batch
+ * with every candidate X, device-resident, one warm-up then `repeats` timed
+ * runs (device time, median), and the fastest X of each class is installed as
+ * the table.  chosen_dc[num_classes] receives the choices (0 for a class
+ * without sample texts, which keeps DC39); ms_out[num_classes *
+ * num_candidates] (may be null) the medians in ms (-1 for such a class).  No
+ * counterpart in the reference, whose cli takes --dcx per run. */
+int dcx_autotune_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offsets, uint32_t num_texts,
+                       const uint64_t* class_max_len, uint32_t num_classes, const int* candidates,
+                       uint32_t num_candidates, uint32_t repeats, int* chosen_dc, double* ms_out);
 
 /* Splits a batch of independent texts over `world` GPUs, one process per GPU.
  * The reference splits its single text into equal blocks per rank

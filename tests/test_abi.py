@@ -57,6 +57,10 @@ def test_null_context_rejected():
     assert lib.dcx_build_sa_batch(None, None, None, 0, 0, 32, None, 0) == pkg.DCX_ERR_ARG
     assert lib.dcx_build_lcp(None, None, 0, None, 32, None, 32, 0) == pkg.DCX_ERR_ARG
     assert lib.dcx_build_gsa(None, None, 0, 39, 32, None, 0) == pkg.DCX_ERR_ARG
+    cnt = ctypes.c_uint32()
+    assert lib.dcx_set_batch_dc_table(None, None, None, 0) == pkg.DCX_ERR_ARG
+    assert lib.dcx_get_batch_dc_table(None, None, None, 0, ctypes.byref(cnt)) == pkg.DCX_ERR_ARG
+    assert lib.dcx_autotune_batch(None, None, None, 0, None, 0, None, 0, 1, None, None) == pkg.DCX_ERR_ARG
     primary = ctypes.c_uint64()
     assert lib.dcx_build_bwt(None, None, 0, None, 32, None, ctypes.byref(primary), 0) == pkg.DCX_ERR_ARG
     assert lib.dcx_check_sa(None, None, 0, None, 32, 0, ctypes.byref(ok)) == pkg.DCX_ERR_ARG
