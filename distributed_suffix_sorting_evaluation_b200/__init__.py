@@ -35,6 +35,7 @@ DCX_ERR_CUDA = -6
 DCX_ERR_INTERNAL = -7
 DCX_ERR_BUSY = -8
 DCX_ERR_NOTFOUND = -9
+DCX_ERR_IO = -10
 
 DCX_HOST_PTRS = 0
 DCX_DEVICE_PTRS = 1
@@ -54,6 +55,7 @@ EXPORTED = (
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
     "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
     "dcx_build_gsa", "dcx_set_batch_dc_table", "dcx_get_batch_dc_table", "dcx_autotune_batch",
+    "dcx_write_sa_file", "dcx_read_sa_file", "dcx_check_sa_file",
 )
 
 # serving request states (dcx_serve_poll)
@@ -139,6 +141,9 @@ def load_library(path: str | None = None):
     lib.dcx_set_batch_dc_table.argtypes = [vp, vp, vp, u32]
     lib.dcx_get_batch_dc_table.argtypes = [vp, vp, vp, u32, ctypes.POINTER(u32)]
     lib.dcx_autotune_batch.argtypes = [vp, vp, vp, u32, vp, u32, vp, u32, u32, vp, vp]
+    lib.dcx_write_sa_file.argtypes = [vp, ctypes.c_char_p, vp, u64, i32, u64]
+    lib.dcx_read_sa_file.argtypes = [vp, ctypes.c_char_p, vp, u64, i32, u64]
+    lib.dcx_check_sa_file.argtypes = [vp, vp, u64, ctypes.c_char_p, i32, u32, ctypes.POINTER(i32)]
     _lib = lib
     return lib
 
@@ -363,6 +368,25 @@ class Context:
         _check(self.lib.dcx_build_bwt(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
                                       ctypes.c_void_p(bwt_ptr), ctypes.byref(primary), DCX_DEVICE_PTRS))
         return int(primary.value)
+
+    def write_sa_file(self, path: str, sa_ptr: int, n: int, sa_width: int, chunk_bytes: int = 0):
+        """Device-resident SA -> file in the reference's raw layout (streamed)."""
+        _check(self.lib.dcx_write_sa_file(self.h, os.fsencode(path), ctypes.c_void_p(sa_ptr), n, sa_width,
+                                          chunk_bytes))
+
+    def read_sa_file(self, path: str, sa_ptr: int, n: int, sa_width: int, chunk_bytes: int = 0):
+        """SA file in the reference's raw layout -> device memory (streamed)."""
+        _check(self.lib.dcx_read_sa_file(self.h, os.fsencode(path), ctypes.c_void_p(sa_ptr), n, sa_width,
+                                         chunk_bytes))
+
+    def check_sa_file(self, text, path: str, sa_width: int) -> bool:
+        """GPU check of the SA stored in `path` against a host text."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        ok = ctypes.c_int()
+        _check(self.lib.dcx_check_sa_file(self.h, t.ctypes.data if t.size else None, t.size, os.fsencode(path),
+                                          sa_width, DCX_HOST_PTRS, ctypes.byref(ok)))
+        return bool(ok.value)
 
     def check_sa_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int) -> bool:
         """GPU check of a device-resident SA against a device-resident text."""

@@ -7,6 +7,8 @@
 //   compute_sa      cli.cpp:655-689 (alphabet remap + DCX with or without packing)
 //   check_sa        cli.cpp:700-727 (--check prints "SA_ok=1" when correct)
 //   write_sa        cli.cpp:691-698 (--output: raw uint40 little endian, or --sa-width 64)
+//   --sa-input F    (GPU addition) with --check: check the SA in file F, in
+//                   that raw layout, instead of building one
 //   JSON            cli.cpp:804-817 (<path>_timer.json / <path>_counter.json)
 // Flags that tune the distributed sorters or the bucket scheme of the reference
 // (--atomic-sorter, --buckets-*, --splitter-*, ...) are accepted and recorded in
@@ -38,7 +40,7 @@ const std::set<std::string> kValueFlags = {
     "--ams-levels", "--splitter-sampling", "--splitter-sorting", "--string-sorter", "--memory_seq_string_sorter",
     "--lcp-compression-threshold", "--inital-prefix-length",
     // GPU additions
-    "--sa-width", "--device", "--hbm-budget", "--recursion-dc"};
+    "--sa-width", "--device", "--hbm-budget", "--recursion-dc", "--sa-input"};
 const std::set<std::string> kBoolFlags = {
     "--check", "--use-random-sampling-splitters", "--balance-blocks-space-efficient-sort", "--use-randomized-chunks",
     "--use-char-packing-samples", "--use-char-packing-merging", "--rearrange-buckets-balanced", "--use-robust-tie-break",
@@ -52,7 +54,7 @@ const std::set<std::string> kHonoured = {"--input", "--textsize", "--output", "-
                                          "--seed", "--alphabet_size", "--use-char-packing-samples",
                                          "--use-char-packing-merging", "--discarding-threshold", "--pack-extra-words",
                                          "--iteration", "--sa-width", "--device", "--hbm-budget", "--recursion-dc",
-                                         "--dry-run"};
+                                         "--dry-run", "--sa-input"};
 
 struct Args {
     std::map<std::string, std::string> v;
@@ -155,6 +157,7 @@ int main(int argc, char** argv) {
     if (a.get("--pack-extra-words", "0") != "0") return fail("--pack-extra-words: only 0 is supported (cli.cpp:675-682)");
     if (!(width == 32 || width == 40 || width == 64)) return fail("--sa-width must be 32, 40 or 64");
     if (dcx_dc_table(X, nullptr, nullptr, nullptr, nullptr) != DCX_OK) return fail("unsupported --dcx " + dcx);
+    if (a.has("--sa-input") && !a.has("--check")) return fail("--sa-input needs --check");
 
     std::vector<std::pair<std::string, std::string>> config;
     for (auto& kv : a.v) config.emplace_back(kv.first.substr(2), kv.second);
@@ -203,6 +206,20 @@ int main(int argc, char** argv) {
     dcx_ctx* ctx = nullptr;
     int rc = dcx_ctx_create(&ctx, device, std::stoull(a.get("--hbm-budget", "0")));
     if (rc != DCX_OK) return fail(std::string("dcx_ctx_create: ") + dcx_strerror(rc));
+    // ---- --sa-input: check an existing SA file (e.g. the reference cli's --output) instead of building
+    const std::string sa_input = a.get("--sa-input");
+    if (!sa_input.empty()) {
+        int ok = 0;
+        auto c0 = std::chrono::steady_clock::now();
+        rc = dcx_check_sa_file(ctx, text.data(), n, sa_input.c_str(), width, DCX_HOST_PTRS, &ok);
+        const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
+        dcx_ctx_destroy(ctx);
+        if (rc != DCX_OK) return fail(std::string("dcx_check_sa_file: ") + dcx_strerror(rc));
+        std::cout << (ok ? "Correct SA!" : "ERROR: Not a correct SA!") << "\n";
+        std::cout << "SA_ok=" << ok << "\n";
+        std::cout << "check_time=" << s << "\n";
+        return 0;
+    }
     dcx_set_option(ctx, "discarding_threshold", discarding);
     if (a.has("--recursion-dc")) dcx_set_option(ctx, "recursion_dc", std::stod(a.get("--recursion-dc")));
     std::vector<uint8_t> sa(n * (width / 8) + 1);

@@ -1686,6 +1686,117 @@ static bool check_one(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     return d2h_scalar(c, bad.get()) == 0;
 }
 
+// ---------------------------------------------------------------------------
+// SA files in the reference's raw layout: the entries back to back, little
+// endian, no header (write_data, lightweight_dcx/src/mpi/io.hpp:80-98; 40-bit
+// entries are util/uint_types.hpp's uint40).  Device <-> file through two
+// pinned chunk buffers, so the copy of one chunk overlaps the file access of
+// the other.
+// ---------------------------------------------------------------------------
+struct ChunkStage {
+    cudaStream_t stream = nullptr;
+    void* buf[2] = {};
+    cudaEvent_t done[2] = {};
+    FILE* f = nullptr;
+    ~ChunkStage() {
+        if (stream) cudaStreamSynchronize(stream);  // no copy may still target the buffers
+        for (int b = 0; b < 2; b++) {
+            if (buf[b]) cudaFreeHost(buf[b]);
+            if (done[b]) cudaEventDestroy(done[b]);
+        }
+        if (f) fclose(f);
+    }
+};
+
+static uint64_t sa_file_chunk(uint64_t total, uint64_t chunk) {
+    if (chunk == 0) chunk = 64ull << 20;
+    return std::max<uint64_t>(std::min<uint64_t>(chunk, total), 1);
+}
+
+static void open_stage(Ctx& c, ChunkStage& cs, const char* path, const char* mode, uint64_t chunk) {
+    cs.f = fopen(path, mode);
+    if (!cs.f) throw Error(DCX_ERR_IO, std::string("cannot open ") + path);
+    cs.stream = c.stream;
+    for (int b = 0; b < 2; b++) {
+        DCX_CUDA(cudaHostAlloc(&cs.buf[b], chunk, cudaHostAllocDefault));
+        DCX_CUDA(cudaEventCreateWithFlags(&cs.done[b], cudaEventDisableTiming));
+    }
+}
+
+static void write_sa_file(Ctx& c, const char* path, const void* sa_dev, uint64_t n, int width, uint64_t chunk) {
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (!path || (n && !sa_dev)) throw Error(DCX_ERR_ARG, "null pointer");
+    const uint64_t total = n * (uint64_t)(width / 8);
+    chunk = sa_file_chunk(total, chunk);
+    ChunkStage cs;
+    open_stage(c, cs, path, "wb", chunk);
+    const uint64_t chunks = div_up(total, chunk);
+    auto len_of = [&](uint64_t i) { return std::min<uint64_t>(chunk, total - i * chunk); };
+    for (uint64_t i = 0; i < chunks; i++) {
+        const int b = (int)(i & 1);
+        // buffer b last held chunk i-2, written to the file in the previous iteration
+        DCX_CUDA(cudaMemcpyAsync(cs.buf[b], (const uint8_t*)sa_dev + i * chunk, len_of(i), cudaMemcpyDeviceToHost,
+                                 c.stream));
+        DCX_CUDA(cudaEventRecord(cs.done[b], c.stream));
+        if (i > 0) {
+            DCX_CUDA(cudaEventSynchronize(cs.done[b ^ 1]));
+            if (fwrite(cs.buf[b ^ 1], 1, len_of(i - 1), cs.f) != len_of(i - 1))
+                throw Error(DCX_ERR_IO, std::string("short write to ") + path);
+        }
+    }
+    if (chunks) {
+        const int b = (int)((chunks - 1) & 1);
+        DCX_CUDA(cudaEventSynchronize(cs.done[b]));
+        if (fwrite(cs.buf[b], 1, len_of(chunks - 1), cs.f) != len_of(chunks - 1))
+            throw Error(DCX_ERR_IO, std::string("short write to ") + path);
+    }
+    FILE* f = cs.f;
+    cs.f = nullptr;
+    if (fclose(f) != 0) throw Error(DCX_ERR_IO, std::string("cannot close ") + path);
+}
+
+static void read_sa_file(Ctx& c, const char* path, void* sa_dev, uint64_t n, int width, uint64_t chunk) {
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (!path || (n && !sa_dev)) throw Error(DCX_ERR_ARG, "null pointer");
+    const uint64_t total = n * (uint64_t)(width / 8);
+    chunk = sa_file_chunk(total, chunk);
+    ChunkStage cs;
+    open_stage(c, cs, path, "rb", chunk);
+    if (fseeko(cs.f, 0, SEEK_END) != 0) throw Error(DCX_ERR_IO, std::string("cannot seek in ") + path);
+    const off_t size = ftello(cs.f);
+    if (size < 0 || (uint64_t)size < total) throw Error(DCX_ERR_ARG, "SA file shorter than n entries");
+    rewind(cs.f);
+    const uint64_t chunks = div_up(total, chunk);
+    for (uint64_t i = 0; i < chunks; i++) {
+        const int b = (int)(i & 1);
+        const uint64_t len = std::min<uint64_t>(chunk, total - i * chunk);
+        if (i >= 2) DCX_CUDA(cudaEventSynchronize(cs.done[b]));  // the copy of chunk i-2 left buffer b
+        if (fread(cs.buf[b], 1, len, cs.f) != len) throw Error(DCX_ERR_IO, std::string("short read of ") + path);
+        DCX_CUDA(cudaMemcpyAsync((uint8_t*)sa_dev + i * chunk, cs.buf[b], len, cudaMemcpyHostToDevice, c.stream));
+        DCX_CUDA(cudaEventRecord(cs.done[b], c.stream));
+    }
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// dcx_check_sa for an SA file: the file streamed into device memory, the text
+// (host or device per flags) beside it.
+static bool check_sa_file(Ctx& c, const uint8_t* text, uint64_t n, const char* path, int width, uint32_t flags) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (!path || (n && !text)) throw Error(DCX_ERR_ARG, "null pointer");
+    DBuf<uint8_t> dsa(&c, std::max<uint64_t>(n * (width / 8), 1));
+    read_sa_file(c, path, dsa.get(), n, width, 0);
+    if (n == 0) return true;
+    const uint8_t* dtext = text;
+    DBuf<uint8_t> t;
+    if (!(flags & DCX_DEVICE_PTRS)) {
+        t = DBuf<uint8_t>(&c, n);
+        DCX_CUDA(cudaMemcpyAsync(t.get(), text, n, cudaMemcpyHostToDevice, c.stream));
+        dtext = t.get();
+    }
+    return check_one(c, dtext, n, dsa.get(), width, DCX_DEVICE_PTRS);
+}
+
 // LCP (or PLCP with DCX_LCP_PERMUTED) of a text and its SA; lcp_width 32 or 64.
 static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, int sa_width, void* out,
                       int lcp_width, uint32_t flags) {
@@ -1973,6 +2084,7 @@ const char* dcx_strerror(int code) {
         case DCX_ERR_INTERNAL: return "internal error";
         case DCX_ERR_BUSY: return "busy";
         case DCX_ERR_NOTFOUND: return "unknown request";
+        case DCX_ERR_IO: return "file error";
         default: return "unknown error";
     }
 }
@@ -2123,6 +2235,35 @@ int dcx_check_sa(dcx_ctx* x, const uint8_t* text, uint64_t n, const void* sa, in
         std::lock_guard<std::mutex> lk(x->c.build_mu);
         DCX_CUDA(cudaSetDevice(x->c.device));
         *ok = dcx::check_one(x->c, text, n, sa, sa_width, flags) ? 1 : 0;
+    });
+}
+
+int dcx_write_sa_file(dcx_ctx* x, const char* path, const void* sa_dev, uint64_t n, int sa_width,
+                      uint64_t chunk_bytes) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::write_sa_file(x->c, path, sa_dev, n, sa_width, chunk_bytes);
+    });
+}
+
+int dcx_read_sa_file(dcx_ctx* x, const char* path, void* sa_dev, uint64_t n, int sa_width, uint64_t chunk_bytes) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::read_sa_file(x->c, path, sa_dev, n, sa_width, chunk_bytes);
+    });
+}
+
+int dcx_check_sa_file(dcx_ctx* x, const uint8_t* text, uint64_t n, const char* path, int sa_width, uint32_t flags,
+                      int* ok) {
+    if (!x || !ok) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        *ok = dcx::check_sa_file(x->c, text, n, path, sa_width, flags) ? 1 : 0;
     });
 }
 

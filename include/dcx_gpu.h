@@ -38,6 +38,7 @@ extern "C" {
 #define DCX_ERR_INTERNAL (-7) /* internal consistency check failed */
 #define DCX_ERR_BUSY (-8)     /* serving queue full or request not finished */
 #define DCX_ERR_NOTFOUND (-9) /* unknown serving request id */
+#define DCX_ERR_IO (-10)      /* a file could not be opened, read or written */
 
 /* ---- flags for dcx_build_sa / dcx_build_sa_batch ---------------------------- */
 #define DCX_HOST_PTRS 0u        /* text / sa_out are host pointers (pinned or pageable) */
@@ -112,6 +113,25 @@ int dcx_build_sa_strict(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, i
  * wired to `cli --check`, cli.cpp:700-727).  *ok = 1 if correct, 0 if not. */
 int dcx_check_sa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
                  uint32_t flags, int* ok);
+
+/* ---- SA files ---------------------------------------------------------------- */
+/* The reference writes an SA as its entries back to back, little endian, no
+ * header (write_data, lightweight_dcx/src/mpi/io.hpp:80-98; uint40 entries,
+ * util/uint_types.hpp:49-269).  These move such a file between the disk and
+ * device memory without a host copy of the whole SA: two pinned buffers of
+ * chunk_bytes (0 = 64 MiB), the device<->host copy of one chunk overlapping the
+ * file access of the other.  dcx_read_sa_file returns DCX_ERR_ARG for a file
+ * shorter than n entries (longer files are read from the start);
+ * DCX_ERR_IO when the file cannot be opened, read or written. */
+int dcx_write_sa_file(dcx_ctx* ctx, const char* path, const void* sa_dev, uint64_t n, int sa_width,
+                      uint64_t chunk_bytes);
+int dcx_read_sa_file(dcx_ctx* ctx, const char* path, void* sa_dev, uint64_t n, int sa_width,
+                     uint64_t chunk_bytes);
+/* dcx_check_sa for an SA stored in such a file (e.g. the --output of the
+ * reference's cli): the file is streamed to the device and checked there; the
+ * text is a host or device pointer per flags.  *ok as for dcx_check_sa. */
+int dcx_check_sa_file(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const char* path, int sa_width,
+                      uint32_t flags, int* ok);
 
 /* ---- LCP ------------------------------------------------------------------- */
 /* Longest-common-prefix array of a text and its suffix array (sa_width 32, 40

@@ -94,3 +94,14 @@ def test_checker_accepts_and_rejects(ctx, oracle):
     dup = sa.copy()
     dup[7] = dup[8]
     assert not ctx.check_sa(t, dup, 64)
+
+
+def test_sa_input_flag(cli, tmp_path):
+    f = tmp_path / "t.bin"
+    f.write_bytes(b"ACGT" * 10)
+    sa = str(tmp_path / "t.sa")
+    r = run(cli, "--input", str(f), "--dcx", "dc3", "--sa-input", sa, "--check", "--dry-run")
+    assert r.returncode == 0, r.stderr
+    assert "--sa-input" not in json.loads(r.stdout)["ignored"]
+    r = run(cli, "--input", str(f), "--dcx", "dc3", "--sa-input", sa, "--dry-run")
+    assert r.returncode == 1 and "needs --check" in r.stderr
