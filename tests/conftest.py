@@ -15,6 +15,26 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libdcxgpu.so")
 
 
+# Suites run in dependency order: the suffix-array build itself first, then
+# what wraps it (batches, serving, the CLI), then what consumes its output
+# (LCP, SA files, BWT, generalized SA) and the batched-DC tuning; the
+# allocation-free entry point last, in a file of its own.  Under -x a failure
+# in a consumer then never hides the state of the build it consumes.
+_SUITE_ORDER = ["test_abi", "test_oracle", "test_golden_fixtures", "test_gpu_parity", "test_gpu_batch",
+                "test_gpu_serve", "test_cli", "test_gpu_lcp", "test_gpu_safile", "test_gpu_bwt", "test_gpu_gsa",
+                "test_gpu_batch_autotune"]
+
+
+def pytest_collection_modifyitems(config, items):
+    def rank(item):
+        name = os.path.splitext(os.path.basename(str(item.fspath)))[0]
+        if name == "test_zz_no_alloc":
+            return len(_SUITE_ORDER) + 1
+        return _SUITE_ORDER.index(name) if name in _SUITE_ORDER else len(_SUITE_ORDER)
+
+    items.sort(key=rank)  # stable: the order inside a file is kept
+
+
 def gpu_available() -> bool:
     try:
         import torch
