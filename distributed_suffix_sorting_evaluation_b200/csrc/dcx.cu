@@ -477,6 +477,10 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // A look-back wait that gave up leaves the order wrong but every write in
+    // range (the scatter checks its destinations); stop here with
+    // DCX_ERR_TIMEOUT, before any kernel uses the sorted values as indices.
+    check_device_error(c);
     c.st.ms_radix += ms;
     c.launched(run.size());
     c.st.radix_passes += run.size();
