@@ -72,6 +72,12 @@ extern "C" int kshim_gsa(const uint8_t* text, uint64_t n, const uint32_t* plain_
     return 0;
 }
 
+// The SA of any width to uint32 (k_sa_to_u32: 40-bit entries four at a time).
+extern "C" int kshim_sa_to_u32(const void* sa, int width, uint64_t n, uint32_t* out) {
+    LAUNCH(k_sa_to_u32, G, B, sa, width, n, out);
+    return 0;
+}
+
 extern "C" int kshim_lcp(const uint8_t* text, uint64_t n, const uint32_t* sa, int gsa, uint32_t* lcp_out) {
     if (n == 0) return 0;
     uint8_t* t = padded(text, n);

@@ -42,6 +42,7 @@ def kh(tmp_path_factory):
     lib.kshim_bwt.argtypes = [vp, u64, vp, ctypes.c_int, vp, ctypes.POINTER(u64)]
     lib.kshim_gsa.argtypes = [vp, u64, vp, vp]
     lib.kshim_lcp.argtypes = [vp, u64, vp, ctypes.c_int, vp]
+    lib.kshim_sa_to_u32.argtypes = [vp, ctypes.c_int, u64, vp]
     return lib
 
 
@@ -145,3 +146,18 @@ def test_plain_lcp_kernel(kh, oracle):
         sa = oracle.libsais(t)
         rc, lcp = _lcp(kh, t, sa, False)
         assert rc == 0 and np.array_equal(lcp, oracle.libsais_lcp(t, sa)[1])
+
+
+def test_sa_width_decode_kernel(kh):
+    """k_sa_to_u32 (the LCP path's reader of 32/40/64-bit SAs; 40-bit entries
+    four at a time from aligned words, the tail one by one)."""
+    rng = np.random.default_rng(10)
+    for n in (1, 2, 3, 4, 5, 7, 8, 9, 1000, 4097):
+        sa = rng.permutation(n).astype(np.uint64) + np.uint64(rng.integers(0, 1 << 31))
+        for width in (32, 40, 64):
+            raw = _pack(sa, width)
+            buf = np.zeros(raw.size + 8, np.uint8)  # 8-byte aligned base, as device buffers are
+            buf[: raw.size] = raw
+            out = np.zeros(n, np.uint32)
+            kh.kshim_sa_to_u32(buf.ctypes.data, width, n, out.ctypes.data)
+            assert np.array_equal(out, sa.astype(np.uint32)), (n, width)
