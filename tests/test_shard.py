@@ -70,3 +70,19 @@ def test_deterministic():
     a, _ = shard_texts(lens, 8)
     b, _ = shard_texts(lens.copy(), 8)
     assert np.array_equal(a, b)
+
+
+def test_bench_batch_chunks_and_share():
+    """bench.py's chunking of a rank's texts (consecutive runs of about `cap`
+    bytes, a longer text alone) and its share of the batch at N = 1."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    lens = np.array([5, 5, 20, 1, 1, 1, 7], np.int64)
+    chunks = bench.batch_chunks(lens, 10)
+    assert chunks == [(0, 2, 10), (2, 3, 20), (3, 7, 10)]
+    assert sum(c[2] for c in chunks) == int(lens.sum())
+    assert bench.batch_chunks(np.zeros(0, np.int64), 10) == []
+    ids, shift, job, steps = bench.batch_share(lens, 1, 0, 10)
+    assert ids.tolist() == list(range(lens.size)) and shift == 0 and job == int(lens.sum()) and steps == 3
