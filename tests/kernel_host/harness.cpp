@@ -72,6 +72,12 @@ extern "C" int kshim_gsa(const uint8_t* text, uint64_t n, const uint32_t* plain_
     return 0;
 }
 
+// uint32 SA entries written at any width (k_store_sa / store_sa_entry).
+extern "C" int kshim_store_sa(const uint32_t* sa32, uint64_t n, void* out, int width) {
+    LAUNCH(k_store_sa, G, B, sa32, n, out, width);
+    return 0;
+}
+
 // The SA of any width to uint32 (k_sa_to_u32: 40-bit entries four at a time).
 extern "C" int kshim_sa_to_u32(const void* sa, int width, uint64_t n, uint32_t* out) {
     LAUNCH(k_sa_to_u32, G, B, sa, width, n, out);

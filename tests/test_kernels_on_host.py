@@ -43,6 +43,7 @@ def kh(tmp_path_factory):
     lib.kshim_gsa.argtypes = [vp, u64, vp, vp]
     lib.kshim_lcp.argtypes = [vp, u64, vp, ctypes.c_int, vp]
     lib.kshim_sa_to_u32.argtypes = [vp, ctypes.c_int, u64, vp]
+    lib.kshim_store_sa.argtypes = [vp, u64, vp, ctypes.c_int]
     return lib
 
 
@@ -161,3 +162,7 @@ def test_sa_width_decode_kernel(kh):
             out = np.zeros(n, np.uint32)
             kh.kshim_sa_to_u32(buf.ctypes.data, width, n, out.ctypes.data)
             assert np.array_equal(out, sa.astype(np.uint32)), (n, width)
+            s32 = np.ascontiguousarray(sa.astype(np.uint32))
+            back = np.zeros(raw.size, np.uint8)
+            kh.kshim_store_sa(s32.ctypes.data, n, back.ctypes.data, width)
+            assert back.tobytes() == raw.tobytes(), (n, width)
