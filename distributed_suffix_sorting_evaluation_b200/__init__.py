@@ -55,7 +55,7 @@ EXPORTED = (
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
     "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
     "dcx_build_gsa", "dcx_set_batch_dc_table", "dcx_get_batch_dc_table", "dcx_autotune_batch",
-    "dcx_write_sa_file", "dcx_read_sa_file", "dcx_check_sa_file",
+    "dcx_write_sa_file", "dcx_read_sa_file", "dcx_check_sa_file", "dcx_bwt",
 )
 
 # serving request states (dcx_serve_poll)
@@ -137,6 +137,7 @@ def load_library(path: str | None = None):
     lib.dcx_check_sa.argtypes = [vp, vp, u64, vp, i32, u32, ctypes.POINTER(i32)]
     lib.dcx_shard_texts.argtypes = [vp, u32, u32, vp, vp]
     lib.dcx_build_bwt.argtypes = [vp, vp, u64, vp, i32, vp, ctypes.POINTER(u64), u32]
+    lib.dcx_bwt.argtypes = [vp, vp, vp, u64, i32, ctypes.POINTER(u64), u32]
     lib.dcx_build_gsa.argtypes = [vp, vp, u64, i32, i32, vp, u32]
     lib.dcx_set_batch_dc_table.argtypes = [vp, vp, vp, u32]
     lib.dcx_get_batch_dc_table.argtypes = [vp, vp, vp, u32, ctypes.POINTER(u32)]
@@ -360,6 +361,16 @@ class Context:
         _check(self.lib.dcx_build_bwt(self.h, t.ctypes.data if t.size else None, t.size,
                                       s.ctypes.data if s.size else None, 64, out.ctypes.data,
                                       ctypes.byref(primary), DCX_HOST_PTRS))
+        return out[: t.size], int(primary.value)
+
+    def bwt(self, text, dc: int = 39):
+        """(BWT, primary index) of a host text, SA built on the GPU: libsais64_bwt's result."""
+        t = np.ascontiguousarray(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else np.asarray(text, dtype=np.uint8))
+        out = np.zeros(max(t.size, 1), np.uint8)
+        primary = ctypes.c_uint64()
+        _check(self.lib.dcx_bwt(self.h, t.ctypes.data if t.size else None, out.ctypes.data, t.size, dc,
+                                ctypes.byref(primary), DCX_HOST_PTRS))
         return out[: t.size], int(primary.value)
 
     def build_bwt_device(self, text_ptr: int, n: int, sa_ptr: int, sa_width: int, bwt_ptr: int) -> int:

@@ -1896,6 +1896,33 @@ static uint64_t build_bwt(Ctx& c, const uint8_t* text, uint64_t n, const void* s
     return p;
 }
 
+// BWT of a text, its SA built on the GPU and dropped (libsais64_bwt's call).
+static uint64_t bwt_of_text(Ctx& c, const uint8_t* text, uint64_t n, int X, uint8_t* out, uint32_t flags) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "text longer than 2^32 - 2");
+    get_dc(c, (uint32_t)X);
+    if (n == 0) return 0;
+    if (!text || !out) throw Error(DCX_ERR_ARG, "null pointer");
+    const bool dev = flags & DCX_DEVICE_PTRS;
+    DBuf<uint8_t> t, o;
+    const uint8_t* dtext = text;
+    uint8_t* dout = out;
+    if (!dev) {
+        t = DBuf<uint8_t>(&c, n + 16, true);
+        o = DBuf<uint8_t>(&c, n, true);
+        DCX_CUDA(cudaMemcpyAsync(t.get(), text, n, cudaMemcpyHostToDevice, c.stream));
+        dtext = t.get();
+        dout = o.get();
+    }
+    DBuf<uint32_t> sa32(&c, n);
+    build_one(c, dtext, n, X, 32, sa32.get(), DCX_DEVICE_PTRS | (flags & DCX_NO_PACKING), false);
+    const uint64_t p = build_bwt(c, dtext, n, sa32.get(), 32, dout, DCX_DEVICE_PTRS);
+    if (!dev) {
+        DCX_CUDA(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, c.stream));
+        DCX_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    return p;
+}
+
 // Generalized SA of a string set (libsais64_gsa convention) from the plain SA:
 // runs of plain-SA neighbours that agree through their separators re-sorted by
 // position.
@@ -2219,6 +2246,16 @@ int dcx_build_gsa(dcx_ctx* x, const uint8_t* text, uint64_t n, int dc, int w, vo
         std::lock_guard<std::mutex> lk(x->c.build_mu);
         DCX_CUDA(cudaSetDevice(x->c.device));
         dcx::build_gsa(x->c, text, n, dc, w, out, flags);
+    });
+}
+
+int dcx_bwt(dcx_ctx* x, const uint8_t* text, uint8_t* bwt_out, uint64_t n, int dc, uint64_t* primary_index,
+            uint32_t flags) {
+    if (!x || !primary_index) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        *primary_index = dcx::bwt_of_text(x->c, text, n, dc, bwt_out, flags);
     });
 }
 

@@ -173,6 +173,11 @@ int dcx_build_gsa(dcx_ctx* ctx, const uint8_t* text, uint64_t n, int dc, int sa_
  * dcx_check_sa does that).  Host or device pointers as for dcx_build_sa. */
 int dcx_build_bwt(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa, int sa_width,
                   uint8_t* bwt_out, uint64_t* primary_index, uint32_t flags);
+/* The same BWT straight from the text, as libsais64_bwt(T, U, A, n, 0, NULL)
+ * returns it: the SA is built on the GPU with difference cover `dc` and not
+ * returned.  Host or device pointers as for dcx_build_sa. */
+int dcx_bwt(dcx_ctx* ctx, const uint8_t* text, uint8_t* bwt_out, uint64_t n, int dc, uint64_t* primary_index,
+            uint32_t flags);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
  * caller can time builds with events recorded on it. */

@@ -63,6 +63,7 @@ def test_null_context_rejected():
     assert lib.dcx_autotune_batch(None, None, None, 0, None, 0, None, 0, 1, None, None) == pkg.DCX_ERR_ARG
     primary = ctypes.c_uint64()
     assert lib.dcx_build_bwt(None, None, 0, None, 32, None, ctypes.byref(primary), 0) == pkg.DCX_ERR_ARG
+    assert lib.dcx_bwt(None, None, None, 0, 39, ctypes.byref(primary), 0) == pkg.DCX_ERR_ARG
     assert lib.dcx_check_sa(None, None, 0, None, 32, 0, ctypes.byref(ok)) == pkg.DCX_ERR_ARG
     assert lib.dcx_serve_submit(None, None, 0, 0, 32, ctypes.byref(rid)) == pkg.DCX_ERR_ARG
     assert lib.dcx_serve_submit_ex(None, None, 0, 0, 32, 0, ctypes.byref(rid)) == pkg.DCX_ERR_ARG

@@ -62,3 +62,13 @@ def test_bwt_refuses_what_is_not_a_suffix_array(ctx, oracle):
     got, q = ctx.build_bwt(t, sa)      # the context is still usable
     want, p = oracle.libsais_bwt(t)
     assert q == p and np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("idx", [1, 2, 3, 6, 9, 10])
+def test_bwt_from_text_like_libsais(ctx, oracle, idx):
+    """dcx_bwt: text in, BWT and primary index out, as libsais64_bwt."""
+    t = _cases()[idx]
+    want, p = oracle.libsais_bwt(t)
+    for dc in (3, 39):
+        got, q = ctx.bwt(t, dc=dc)
+        assert q == p and np.array_equal(got, want)
