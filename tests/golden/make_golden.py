@@ -1,10 +1,15 @@
-"""Generates tests/golden/sa_lcp_fixtures.npz: seeded texts with the suffix
-array and LCP array computed by libsais 2.10 compiled from the reference
-tree's own sources (oracle/_ref/libsais.so, built by oracle/Makefile).
+"""Generates the committed fixtures, computed by libsais 2.10 compiled from the
+reference tree's own sources (oracle/_ref/libsais.so, built by oracle/Makefile):
+
+  sa_lcp_fixtures.npz   seeded texts with their suffix array and LCP array;
+  bwt_gsa_fixtures.npz  the same texts' BWT (libsais64_bwt: U and the primary
+                        index), and seeded 0-separated string sets with their
+                        generalized SA (libsais64_gsa) and its LCP
+                        (libsais64_plcp_gsa + libsais64_lcp).
 
 The fixtures travel with the repository, so the GPU tests can check against
 reference-computed answers on a machine without the reference tree.  Run from
-the repository root:  python tests/golden/make_golden.py
+the repository root:  python tests/golden/make_golden.py [sa_lcp|bwt_gsa]
 """
 import os
 import sys
@@ -35,6 +40,36 @@ def cases():
     return out
 
 
+def string_sets():
+    rng = np.random.default_rng(20261204)
+    sets = {"psac_tiny": [b"abab", b"baba"]}  # psac/test/test_gsa.cpp:71-101
+    sets["copies"] = [b"ACGTACGTTT"] * 6 + [b"ACGTACG", b"TT"]
+    base = rng.integers(65, 69, 400).astype(np.uint8).tobytes()
+    sets["tails"] = [base[int(rng.integers(0, 400)):] for _ in range(30)] + [base[: int(rng.integers(1, 400))]
+                                                                          for _ in range(30)]
+    sets["random"] = [rng.integers(97, 101, int(rng.integers(1, 300))).astype(np.uint8).tobytes()
+                      for _ in range(200)]
+    return {k: np.frombuffer(b"".join(s + b"\0" for s in v), np.uint8).copy() for k, v in sets.items()}
+
+
+def main_bwt_gsa():
+    arrays = {}
+    for name, t in cases().items():
+        u, p = O.libsais_bwt(t)
+        arrays[f"text_{name}"] = t
+        arrays[f"bwt_{name}"] = u
+        arrays[f"primary_{name}"] = np.array([p], np.uint64)
+    for name, t in string_sets().items():
+        g = O.libsais_gsa(t)
+        _, lcp = O.libsais_lcp_gsa(t, g)
+        arrays[f"set_{name}"] = t
+        arrays[f"gsa_{name}"] = g.astype(np.uint32)
+        arrays[f"glcp_{name}"] = lcp.astype(np.uint32)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bwt_gsa_fixtures.npz")
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path}")
+
+
 def main():
     arrays = {}
     for name, t in cases().items():
@@ -49,4 +84,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if which in ("all", "sa_lcp"):
+        main()
+    if which in ("all", "bwt_gsa"):
+        main_bwt_gsa()

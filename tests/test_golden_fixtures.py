@@ -46,3 +46,39 @@ def test_gpu_batch_and_lcp_match_fixtures(ctx):
     for (name, t, sa, lcp), g in zip(fx, got):
         assert np.array_equal(g, sa), name
         assert np.array_equal(ctx.build_lcp(t, sa), lcp), name
+
+
+FIX2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bwt_gsa_fixtures.npz")
+
+
+def _bwt_fixtures():
+    with np.load(FIX2) as z:
+        names = sorted(k[len("bwt_"):] for k in z.files if k.startswith("bwt_"))
+        return [(n, z["text_" + n], z["bwt_" + n], int(z["primary_" + n][0])) for n in names]
+
+
+def _gsa_fixtures():
+    with np.load(FIX2) as z:
+        names = sorted(k[len("set_"):] for k in z.files if k.startswith("set_"))
+        return [(n, z["set_" + n], z["gsa_" + n].astype(np.uint64), z["glcp_" + n].astype(np.uint64))
+                for n in names]
+
+
+def test_bwt_gsa_fixtures_against_restatements(oracle):
+    """The BWT fixtures follow from the SA fixtures by the SA-based rule the GPU
+    uses, and the generalized-SA fixtures from the plain SA by the regrouping the
+    GPU uses; the locally built libsais still gives the same answers."""
+    sa_of = {n: sa for n, _, sa, _ in _fixtures()}
+    bw = _bwt_fixtures()
+    assert len(bw) == 11
+    for name, t, u, p in bw:
+        u2, p2 = oracle.bwt_from_sa(t, sa_of[name].astype(np.int64))
+        assert p2 == p and np.array_equal(u2, u), name
+        u3, p3 = oracle.libsais_bwt(t)
+        assert p3 == p and np.array_equal(u3, u), name
+    gs = _gsa_fixtures()
+    assert len(gs) == 4
+    for name, t, g, glcp in gs:
+        assert np.array_equal(oracle.gsa_from_sa(t).astype(np.uint64), g), name
+        assert np.array_equal(oracle.libsais_lcp_gsa(t, g.astype(np.int64))[1].astype(np.uint64), glcp), name
+

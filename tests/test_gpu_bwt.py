@@ -72,3 +72,14 @@ def test_bwt_from_text_like_libsais(ctx, oracle, idx):
     for dc in (3, 39):
         got, q = ctx.bwt(t, dc=dc)
         assert q == p and np.array_equal(got, want)
+
+
+def test_gpu_bwt_matches_fixtures(ctx):
+    """The committed BWT fixtures (libsais64_bwt built from the reference tree)."""
+    from test_golden_fixtures import _bwt_fixtures, _fixtures
+    sa_of = {n: sa for n, _, sa, _ in _fixtures()}
+    for name, t, u, p in _bwt_fixtures():
+        got, q = ctx.build_bwt(t, sa_of[name])
+        assert q == p and np.array_equal(got, u), name
+        got, q = ctx.bwt(t, dc=39)
+        assert q == p and np.array_equal(got, u), name

@@ -94,3 +94,14 @@ def test_gsa_lcp_on_the_psac_test_sets(ctx):
         g = ctx.build_gsa(t)
         lcp = ctx.build_lcp(t, g, gsa=True)
         assert lcp[t[g.astype(np.int64)] != 0].tolist() == psac_glcp_case(seq, reps)
+
+
+@pytest.mark.parametrize("dc", [3, 39])
+def test_gpu_gsa_matches_fixtures(ctx, dc):
+    """The committed generalized-SA fixtures (libsais64_gsa and its LCP, built
+    from the reference tree)."""
+    from test_golden_fixtures import _gsa_fixtures
+    for name, t, g, glcp in _gsa_fixtures():
+        got = ctx.build_gsa(t, dc=dc, sa_width=64)
+        assert np.array_equal(got, g), (name, dc)
+        assert np.array_equal(ctx.build_lcp(t, got, gsa=True), glcp), (name, dc)
