@@ -349,6 +349,23 @@ def run_gpu(args, world, rank, local):
                     "call": "dcx_build_bwt, device pointers"}
         del d_bwt
 
+    gsa_line = None
+    if args.gsa:  # generalized SA of the workload text cut into 1 MiB strings (a 0 ends each)
+        d_set = d_text.clone()
+        d_set[(1 << 20) - 1::1 << 20] = 0
+        d_set[n - 1] = 0
+        d_gsa = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
+        ctx.build_gsa_device(d_set.data_ptr(), n, d_gsa.data_ptr(), dc=dc, sa_width=32)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ctx.build_gsa_device(d_set.data_ptr(), n, d_gsa.data_ptr(), dc=dc, sa_width=32)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_gsa = e0.elapsed_time(e1)
+        gsa_line = {"value": round(n / GiB / (ms_gsa / 1000.0), 4), "unit": "GiB/s", "ms": round(ms_gsa, 3),
+                    "call": "dcx_build_gsa, device pointers, 1 MiB strings, uint32 GSA"}
+        del d_set, d_gsa
+
     # end-to-end through the public call with host buffers; the device-resident
     # buffers of the runs above are released first, so the host-pointer build
     # has the device memory a caller of that path would have
@@ -418,6 +435,8 @@ def run_gpu(args, world, rank, local):
             line["lcp"] = lcp_line
         if bwt_line:
             line["bwt"] = bwt_line
+        if gsa_line:
+            line["gsa"] = gsa_line
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             sample = min(n, args.cpu_sample_mib << 20)
@@ -861,6 +880,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
     ap.add_argument("--bwt", action="store_true", help="also time the BWT of the built SA")
+    ap.add_argument("--gsa", action="store_true",
+                    help="also time the generalized SA of the text cut into 1 MiB strings")
     ap.add_argument("--recursion-dc", type=int, default=0, help="difference cover of the recursion levels")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
                     help="context option (dcx_set_option) for the single-text workloads")
