@@ -14,8 +14,9 @@ Metric: SA build GiB/s of input text on 1 B200 (bit-exact output).
 Inputs are larger than L2 (1 GiB vs 126 MB), so no flush is needed between steps.
 
 --impl reference times the CPU reference implementation instead (libsais 2.10
-built from the reference tree, OpenMP over all host threads) on a bounded prefix
-sample of the same text.  N > 1: one process per GPU, each rank builds its own
+built from the reference tree, OpenMP over all host threads) on the same whole
+text (--ref-sample-mib bounds it to a prefix).  The built SA is checked on the
+GPU after the timed region (--no-verify skips it).  N > 1: one process per GPU, each rank builds its own
 text (independent replicas, weak scaling); the reference arm runs on rank 0 only.
 """
 from __future__ import annotations
@@ -37,6 +38,7 @@ sys.path.insert(0, ROOT)
 
 GiB = float(1 << 30)
 DEFAULT_WORKLOAD = "cfg2_dc39_markov_dna_1GiB"
+RADIX_KERNEL = "k_onesweep_st"
 
 
 def _dist():
@@ -67,14 +69,20 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic_per_launch(kernel: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def _traffic_per_launch(kernel: str, alg_bytes_per_launch: float):
+    """DRAM bytes per launch of the dominant kernel.  profiles/traffic.json holds
+    the DRAM read + write bytes per element-word (one carried 32-bit word of one
+    element: a pass reads and writes each once, 8 algorithmic bytes) that a
+    small-case ncu capture of the same kernel measured; a launch here moves
+    alg_bytes_per_launch / 8 element-words."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            j = json.load(f)
-        return j.get(kernel)
-    return None
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        e = json.load(f).get(kernel)
+    if not isinstance(e, dict) or "dram_bytes_per_element_word" not in e:
+        return None
+    return int(e["dram_bytes_per_element_word"] * alg_bytes_per_launch / 8)
 
 
 class ClockSampler:
@@ -136,7 +144,7 @@ class ClockSampler:
 
 
 def cpu_baseline(text: np.ndarray, sample_bytes: int, threads: int):
-    """libsais64_omp (reference tree sources) on a prefix sample of the text."""
+    """libsais64_omp (reference tree sources) on the first `sample_bytes` of the text."""
     from oracle import oracle as O
     s = np.ascontiguousarray(text[:sample_bytes])
     O.libsais(s[: 1 << 20], threads=threads)  # warm the library and threads
@@ -153,7 +161,7 @@ def run_reference(args, world, rank):
     w = W.WORKLOADS[args.workload]
     text = W.make(args.workload)
     threads = os.cpu_count() or 1
-    sample = min(text.size, args.ref_sample_mib << 20)
+    sample = min(text.size, args.ref_sample_mib << 20) if args.ref_sample_mib else text.size
     for _ in range(args.warmup):
         cpu_baseline(text, min(sample, 64 << 20), threads)
     vals = []
@@ -166,10 +174,13 @@ def run_reference(args, world, rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(sample / GiB / value * 1000, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": args.workload, "text_bytes": int(w["n"]), "dc": w["dc"], "sa_width": w["sa_width"]},
+        "config": {"workload": args.workload, "text_bytes": int(w["n"]), "dc": w["dc"], "sa_width": w["sa_width"],
+                   "timed_text_bytes": int(sample), "same_text": bool(sample == text.size)},
         "cpu_baseline": {"value": round(value, 4), "unit": "GiB/s", "cores": threads, "kind": "reference",
-                         "sample": f"libsais64_omp on the first {sample >> 20} MiB of the workload text, "
-                                   f"{threads} threads"},
+                         "sample": (f"libsais64_omp on the whole {sample >> 20} MiB workload text"
+                                    if sample == text.size else
+                                    f"libsais64_omp on the first {sample >> 20} MiB of the workload text")
+                                   + f", {threads} threads"},
         "e2e": {"value": round(value, 4), "unit": "GiB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -186,7 +197,7 @@ def run_reference_batch(args, world, rank):
     from oracle import oracle as O
     lens = W.batch_lengths(args.batch_count, 1 << 10, 16 << 20, seed=5)
     threads = os.cpu_count() or 1
-    cap = args.ref_sample_mib << 20
+    cap = (args.ref_sample_mib or 256) << 20
     texts, tot = [], 0
     for j in range(lens.size):
         if texts and tot + int(lens[j]) > cap:
@@ -229,7 +240,7 @@ def run_reference_serve(args, world, rank):
     offs = (rng.random(lens.size) * (base_n - lens)).astype(np.int64)
     base = W.markov_dna(base_n, seed=2)
     threads = os.cpu_count() or 1
-    cap = args.ref_sample_mib << 20
+    cap = (args.ref_sample_mib or 256) << 20
     k, tot = 0, 0
     while k < lens.size and (k == 0 or tot + int(lens[k]) <= cap):
         tot += int(lens[k])
@@ -255,6 +266,37 @@ def run_reference_serve(args, world, rank):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def gsa_sample_check(d_set, d_gsa, pairs: int, seed: int) -> str:
+    """Checks a generalized SA built on the device: a permutation of 0..n-1
+    (device sort), and `pairs` random adjacent entries in the order of the
+    string-set convention (suffixes compared through their separator, the 0 that
+    ends each string, which is smaller than every character; suffixes equal
+    through their separators ordered by string).  Raises on a violation."""
+    import torch
+    n = d_set.numel()
+    srt, _ = torch.sort(d_gsa.to(torch.int64))
+    if not torch.equal(srt, torch.arange(n, device=srt.device)):
+        raise SystemExit("the generalized SA is not a permutation")
+    del srt
+    t = d_set.cpu().numpy()
+    g = d_gsa.cpu().numpy().astype(np.int64)
+    zpos = np.flatnonzero(t == 0)
+    rng = np.random.default_rng(seed)
+    for k in rng.integers(1, n, pairs):
+        i, j = int(g[k - 1]), int(g[k])
+        ei, ej = int(zpos[np.searchsorted(zpos, i)]), int(zpos[np.searchsorted(zpos, j)])
+        a, b = t[i:ei + 1], t[j:ej + 1]
+        m = min(a.size, b.size)
+        d = np.flatnonzero(a[:m] != b[:m])
+        if d.size:
+            ok = a[d[0]] < b[d[0]]
+        else:  # equal through the shorter one's separator: only possible when both end together
+            ok = a.size == b.size and ei < ej
+        if not ok:
+            raise SystemExit(f"generalized SA out of order at entry {int(k)}")
+    return f"permutation + {pairs} sampled adjacent pairs in order"
 
 
 def run_gpu(args, world, rank, local):
@@ -352,7 +394,10 @@ def run_gpu(args, world, rank, local):
     gsa_line = None
     if args.gsa:  # generalized SA of the workload text cut into 1 MiB strings (a 0 ends each)
         d_set = d_text.clone()
+        d_set[d_set == 0] = 1  # a 0 inside a string would end it early (Zipf texts hold 0 bytes)
         d_set[(1 << 20) - 1::1 << 20] = 0
+        if n >= 2 and (n - 2) % (1 << 20) == (1 << 20) - 1:
+            d_set[n - 2] = 1  # no empty last string
         d_set[n - 1] = 0
         d_gsa = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
         ctx.build_gsa_device(d_set.data_ptr(), n, d_gsa.data_ptr(), dc=dc, sa_width=32)
@@ -362,8 +407,10 @@ def run_gpu(args, world, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
         ms_gsa = e0.elapsed_time(e1)
+        gsa_checked = gsa_sample_check(d_set, d_gsa, pairs=2000, seed=rank)
         gsa_line = {"value": round(n / GiB / (ms_gsa / 1000.0), 4), "unit": "GiB/s", "ms": round(ms_gsa, 3),
-                    "call": "dcx_build_gsa, device pointers, 1 MiB strings, uint32 GSA"}
+                    "call": "dcx_build_gsa, device pointers, 1 MiB strings, uint32 GSA",
+                    "checked": gsa_checked}
         del d_set, d_gsa
 
     # end-to-end through the public call with host buffers; the device-resident
@@ -422,12 +469,14 @@ def run_gpu(args, world, rank, local):
                     "build_ms": e2e_trace},
             "gpu_launches": int(launches),
             "verified": verified,
-            "roofline": {"kernel": "k_onesweep_st (8-bit LSD radix pass)", "bound": "hbm",
+            "roofline": {"kernel": f"{RADIX_KERNEL} (8-bit LSD radix pass)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "bytes_per_launch": int(bytes_radix / max(passes, 1)),
                          "launches": int(passes),
-                         "traffic": _traffic_per_launch("k_onesweep_st")},
+                         "traffic": _traffic_per_launch(RADIX_KERNEL, bytes_radix / max(passes, 1)),
+                         "traffic_source": "profiles/traffic.json (ncu DRAM bytes per element-word of a small-case "
+                                           "capture, scaled to this launch's element-words)"},
             "build_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in s_last.items()},
             "clocks": clock,
         }
@@ -439,11 +488,12 @@ def run_gpu(args, world, rank, local):
             line["gsa"] = gsa_line
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            sample = min(n, args.cpu_sample_mib << 20)
+            sample = min(n, args.cpu_sample_mib << 20) if args.cpu_sample_mib else n
             v, dt = cpu_baseline(host_text.numpy(), sample, threads)
             line["cpu_baseline"] = {"value": round(v, 4), "unit": "GiB/s", "cores": threads, "kind": "reference",
-                                    "sample": f"libsais64_omp on the first {sample >> 20} MiB of the same text "
-                                              f"({dt:.2f} s), {threads} threads"}
+                                    "sample": (f"libsais64_omp on the whole {sample >> 20} MiB text" if sample == n
+                                               else f"libsais64_omp on the first {sample >> 20} MiB of the same text")
+                                              + f" ({dt:.2f} s), {threads} threads"}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
@@ -875,8 +925,10 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--text-mib", type=int, default=0, help="override the text size (profiling captures)")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-sample-mib", type=int, default=256)
-    ap.add_argument("--ref-sample-mib", type=int, default=256)
+    ap.add_argument("--cpu-sample-mib", type=int, default=0,
+                    help="text prefix the CPU baseline builds (0 = the whole text)")
+    ap.add_argument("--ref-sample-mib", type=int, default=0,
+                    help="text prefix the reference arm builds (0 = the whole text; cfg4/cfg5: 256 MiB)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
     ap.add_argument("--bwt", action="store_true", help="also time the BWT of the built SA")
@@ -892,7 +944,8 @@ def main():
     ap.add_argument("--batch-split", default="lpt", choices=["lpt", "replicas"],
                     help="how the batched workload is split over ranks under torchrun")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")
-    ap.add_argument("--verify", action="store_true", help="check the SA (batched: three SAs per chunk) on the GPU")
+    ap.add_argument("--verify", action=argparse.BooleanOptionalAction, default=True,
+                    help="check the SA (batched: three SAs per chunk) on the GPU after the timed region")
     ap.add_argument("--serve-requests", type=int, default=20000, help="request pool of the serving workload")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="open-loop arrival window")
     ap.add_argument("--serve-cap-gib", type=int, default=16, help="text of the closed-loop capacity run")

@@ -203,6 +203,9 @@ struct Options {
     uint32_t prefix_chars = 0;
     int trace = 0;
     uint32_t spin_limit = 1u << 24;
+    // failure-detection test hook: this tile of every radix pass never publishes
+    // its look-back status, so the next tile's bounded wait runs out
+    uint32_t lookback_hold_tile = 0xffffffffu;
     uint64_t batch_round_cap = 0;  // max elements per batch round (0 = from the budget)
     // DC per size class of batched builds with dc_or_auto = 0: (longest text of
     // the class, X), ascending; longer texts and an empty table use DC39
@@ -247,7 +250,7 @@ struct Ctx {
     uint32_t* d_hist = nullptr;     // [16 * RADIX]
     uint32_t* d_base = nullptr;     // [16 * RADIX]
     uint32_t* d_tiles = nullptr;    // [16]
-    uint32_t* d_err = nullptr;      // [1]
+    uint32_t* d_err = nullptr;      // [2]: error bits, look-back give-ups
     unsigned long long* d_h256 = nullptr;
     uint64_t* d_lookback = nullptr;
     size_t lookback_tiles = 0;
@@ -336,10 +339,14 @@ static T d2h_scalar(Ctx& c, const T* dptr) {
     return *h;
 }
 
+// d_err[0]: error bits of the kernels; d_err[1]: CTAs whose look-back wait ran
+// out (counted into the build's statistics).
 static void check_device_error(Ctx& c) {
-    uint32_t e = d2h_scalar(c, c.d_err);
+    const uint64_t v = d2h_scalar(c, reinterpret_cast<const uint64_t*>(c.d_err));
+    const uint32_t e = (uint32_t)v, gave_up = (uint32_t)(v >> 32);
+    if (v) DCX_CUDA(cudaMemsetAsync(c.d_err, 0, 8, c.stream));
+    c.st.lookback_gave_up += gave_up;
     if (e) {
-        DCX_CUDA(cudaMemsetAsync(c.d_err, 0, 4, c.stream));
         if (e & DEV_ERR_TIMEOUT) throw Error(DCX_ERR_TIMEOUT, "a bounded device wait gave up");
         throw Error(DCX_ERR_INTERNAL, "device range check failed");
     }
@@ -467,6 +474,8 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         a.epoch = c.epoch;
         a.err = c.d_err;
         a.spin_limit = c.opt.spin_limit;
+        a.hold_tile = c.opt.lookback_hold_tile;
+        a.gave_up = c.d_err + 1;
         k_onesweep_st<ITEMS><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a, aligned16);
         DCX_CHECK_LAUNCH();
         cur ^= 1;
@@ -708,7 +717,12 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         for (uint32_t w = 0; w < kwt; w++) kk.w[w] = s.k[f][w];
         head = DBuf<uint8_t>(&c, N);
         DCX_CUDA(cudaMemsetAsync(c.d_h256, 0, 8, c.stream));
-        k_heads<<<grid_for(N, 256), 256, 0, c.stream>>>(kk, kwt, N, head.get(), c.d_h256);
+        {
+            const int hg = grid_for(std::max<uint64_t>(N / 16, 1), 256, 148 * 8);
+            if (kwt == 1) k_heads16<1><<<hg, 256, 0, c.stream>>>(kk, N, head.get(), c.d_h256);
+            else if (kwt == 2) k_heads16<2><<<hg, 256, 0, c.stream>>>(kk, N, head.get(), c.d_h256);
+            else k_heads16<3><<<hg, 256, 0, c.stream>>>(kk, N, head.get(), c.d_h256);
+        }
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(N * kwt * 4 + N);
@@ -1914,7 +1928,7 @@ static uint64_t bwt_of_text(Ctx& c, const uint8_t* text, uint64_t n, int X, uint
         dout = o.get();
     }
     DBuf<uint32_t> sa32(&c, n);
-    build_one(c, dtext, n, X, 32, sa32.get(), DCX_DEVICE_PTRS | (flags & DCX_NO_PACKING), false);
+    build_one(c, dtext, n, X, 32, sa32.get(), DCX_DEVICE_PTRS | (flags & (DCX_NO_PACKING | DCX_NO_REMAP)), false);
     const uint64_t p = build_bwt(c, dtext, n, sa32.get(), 32, dout, DCX_DEVICE_PTRS);
     if (!dev) {
         DCX_CUDA(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, c.stream));
@@ -2037,8 +2051,8 @@ static void ctx_init(Ctx& c, int device, uint64_t budget) {
     DCX_CUDA(cudaMalloc(&c.d_hist, 16 * RADIX * 4));
     DCX_CUDA(cudaMalloc(&c.d_base, 16 * RADIX * 4));
     DCX_CUDA(cudaMalloc(&c.d_tiles, 64 * 4));
-    DCX_CUDA(cudaMalloc(&c.d_err, 4));
-    DCX_CUDA(cudaMemset(c.d_err, 0, 4));
+    DCX_CUDA(cudaMalloc(&c.d_err, 8));
+    DCX_CUDA(cudaMemset(c.d_err, 0, 8));
     DCX_CUDA(cudaMalloc(&c.d_h256, 256 * 8));
     DCX_CUDA(cudaHostAlloc((void**)&c.h_pinned, PINNED_WORDS * 4, cudaHostAllocDefault));
     cudaMemPoolProps props{};
@@ -2194,6 +2208,7 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
     } else if (s == "prefix_chars") o.prefix_chars = (uint32_t)value;
     else if (s == "trace") o.trace = value != 0;
     else if (s == "spin_limit") o.spin_limit = (uint32_t)value;
+    else if (s == "lookback_hold_tile") o.lookback_hold_tile = value < 0 ? 0xffffffffu : (uint32_t)value;
     else if (s == "batch_round_cap") o.batch_round_cap = (uint64_t)value;
     else if (s == "serve_lanes") {
         if (value < 1 || value > 16) return DCX_ERR_ARG;

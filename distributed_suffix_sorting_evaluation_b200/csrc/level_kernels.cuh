@@ -156,19 +156,57 @@ struct KeyWords {
     const uint32_t* w[12];
 };
 
-// Head flags of a sorted key array; *ties (zeroed by the caller) receives the
-// number of elements equal to their predecessor.
-__global__ void k_heads(KeyWords k, uint32_t kw, uint64_t N, uint8_t* __restrict__ head,
-                        unsigned long long* __restrict__ ties) {
+// Head flags of a sorted key array of KW words; *ties (zeroed by the caller)
+// receives the number of elements equal to their predecessor.  Each thread
+// takes 16 consecutive elements: 16-byte loads of every key word (arrays and
+// head 16-byte aligned), one more load for the predecessor of the first, and
+// one 16-byte store of the 16 flags; the tail past the last full 16 is scalar.
+template <int KW>
+__global__ __launch_bounds__(256) void k_heads16(KeyWords k, uint64_t N, uint8_t* __restrict__ head,
+                                                 unsigned long long* __restrict__ ties) {
     uint32_t t = 0;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint8_t h = 1;
+    const uint64_t groups = N / 16;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i0 = g * 16;
+        uint32_t diff[16];
+#pragma unroll
+        for (int e = 0; e < 16; e++) diff[e] = 0;
+#pragma unroll
+        for (int w = 0; w < KW; w++) {
+            const uint4* p = reinterpret_cast<const uint4*>(k.w[w] + i0);
+            uint32_t v[17];
+            v[0] = i0 ? __ldg(k.w[w] + i0 - 1) : ~__ldg(k.w[w]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint4 x = __ldg(p + q);
+                v[1 + 4 * q] = x.x;
+                v[2 + 4 * q] = x.y;
+                v[3 + 4 * q] = x.z;
+                v[4 + 4 * q] = x.w;
+            }
+#pragma unroll
+            for (int e = 0; e < 16; e++) diff[e] |= v[e + 1] ^ v[e];
+        }
+        uint32_t out[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+            const uint32_t h = diff[e] != 0;
+            out[e >> 2] |= h << (8 * (e & 3));
+            t += h ^ 1u;
+        }
+        reinterpret_cast<uint4*>(head + i0)[0] = make_uint4(out[0], out[1], out[2], out[3]);
+    }
+    for (uint64_t i = groups * 16 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t h = 1;
         if (i > 0) {
             h = 0;
-            for (uint32_t w = 0; w < kw; w++) h |= k.w[w][i] != k.w[w][i - 1];
+#pragma unroll
+            for (int w = 0; w < KW; w++) h |= k.w[w][i] != k.w[w][i - 1];
         }
-        head[i] = h;
-        t += !h;
+        head[i] = (uint8_t)h;
+        t += h ^ 1u;
     }
     t = __reduce_add_sync(0xffffffffu, t);
     if ((threadIdx.x & 31) == 0 && t) atomicAdd(ties, (unsigned long long)t);

@@ -56,6 +56,8 @@ struct SortPassArgs {
     uint32_t epoch;
     uint32_t* err;
     uint32_t spin_limit;
+    uint32_t hold_tile;           // tile that never publishes its status (0xffffffff: none)
+    uint32_t* gave_up;            // count of CTAs whose look-back wait ran out
 };
 
 // Lanes of the warp holding the same 8-bit digit, from eight ballots, or nine
@@ -107,12 +109,16 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
     __shared__ uint32_t s_tile_excl[RADIX];
     __shared__ uint32_t s_gbase[RADIX];
     __shared__ uint32_t s_scan[THREADS / 32 + 1];
+    __shared__ uint32_t s_gave_up;
     extern __shared__ __align__(16) uint32_t s_dyn[];
     uint32_t* s_exch = s_dyn;           // [TILE]
     uint32_t* s_stage = s_dyn + TILE;   // [kw][TILE]: carried arrays in tile order
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+    if (tid == 0) {
+        s_tile = atomicAdd(a.tile_counter, 1u);
+        s_gave_up = 0;
+    }
     for (int i = tid; i < WARPS * RADIX; i += THREADS) (&s_warp_hist[0][0])[i] = 0;
     __syncthreads();
     const uint64_t tile = s_tile;
@@ -165,7 +171,8 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
             s_warp_hist[w][d] = count;  // exclusive prefix over warps: the warp's running base
             count += t;
         }
-        st_relaxed(a.lookback + tile * RADIX + d, lb_pack(a.epoch, tile == 0 ? 2u : 1u, count));
+        if (tile != a.hold_tile)
+            st_relaxed(a.lookback + tile * RADIX + d, lb_pack(a.epoch, tile == 0 ? 2u : 1u, count));
         uint32_t total;
         s_tile_excl[d] = block_excl_scan<THREADS>(count, s_scan, total);
     }
@@ -212,16 +219,18 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
                 if (k == 0) {
                     if (++spins > a.spin_limit) {
                         atomicOr(a.err, DEV_ERR_TIMEOUT);
+                        s_gave_up = 1;
                         break;
                     }
                     if (spins > 32) __nanosleep(32);
                 }
             }
-            st_relaxed(a.lookback + tile * RADIX + d, lb_pack(a.epoch, 2u, excl + count));
+            if (tile != a.hold_tile) st_relaxed(a.lookback + tile * RADIX + d, lb_pack(a.epoch, 2u, excl + count));
         }
         s_gbase[d] = a.digit_base[d] + excl - s_tile_excl[d];
     }
     __syncthreads();
+    if (tid == 0 && s_gave_up) atomicAdd(a.gave_up, 1u);
 #pragma unroll
     for (int it = 0; it < ITEMS; it++)
         if (dig[it] < RADIX) pos[it] += s_tile_excl[dig[it]];

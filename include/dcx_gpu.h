@@ -76,6 +76,7 @@ typedef struct dcx_stats {
     double level0_reduction;  /* discarding reduction at level 0 */
     uint64_t tie_groups;      /* phase-4 tie groups (all levels) */
     uint64_t tie_elements;    /* elements in phase-4 tie groups (all levels) */
+    uint64_t lookback_gave_up;/* radix-pass CTAs whose bounded look-back wait ran out */
 } dcx_stats;
 
 /* ---- context --------------------------------------------------------------- */
@@ -90,7 +91,13 @@ int dcx_ctx_destroy(dcx_ctx* ctx);
  *   "small_threshold"      (texts up to this length are solved by the in-CTA
  *                           base case; default 2048, max 2048),
  *   "prefix_chars"         (chars in the first radix sort; 0 = auto),
- *   "trace"                (1 = keep level-0 names/unique flags for dcx_get_trace). */
+ *   "trace"                (1 = keep level-0 names/unique flags for dcx_get_trace),
+ *   "spin_limit"           (polls of a radix pass's look-back wait before it gives
+ *                           up: the build then returns DCX_ERR_TIMEOUT and the
+ *                           contents of its output buffer are undefined; default 2^24),
+ *   "lookback_hold_tile"   (failure-detection test hook: this tile of every radix
+ *                           pass never publishes its look-back status, so the next
+ *                           tile's wait runs out; negative = off, the default). */
 int dcx_set_option(dcx_ctx* ctx, const char* name, double value);
 
 /* ---- single text ----------------------------------------------------------- */
@@ -175,7 +182,8 @@ int dcx_build_bwt(dcx_ctx* ctx, const uint8_t* text, uint64_t n, const void* sa,
                   uint8_t* bwt_out, uint64_t* primary_index, uint32_t flags);
 /* The same BWT straight from the text, as libsais64_bwt(T, U, A, n, 0, NULL)
  * returns it: the SA is built on the GPU with difference cover `dc` and not
- * returned.  Host or device pointers as for dcx_build_sa. */
+ * returned.  Host or device pointers as for dcx_build_sa; DCX_NO_PACKING and
+ * DCX_NO_REMAP act on the SA build as they do there. */
 int dcx_bwt(dcx_ctx* ctx, const uint8_t* text, uint8_t* bwt_out, uint64_t n, int dc, uint64_t* primary_index,
             uint32_t flags);
 

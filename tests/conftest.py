@@ -8,7 +8,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# The reference tree (read in place for its golden files); DCX_REFERENCE_TREE
+# points elsewhere when it is mounted at another path.
+REFERENCE = os.environ.get("DCX_REFERENCE_TREE", "/root/reference")
 
 
 def pytest_configure(config):
@@ -22,7 +24,7 @@ def pytest_configure(config):
 # in a consumer then never hides the state of the build it consumes.
 _SUITE_ORDER = ["test_abi", "test_oracle", "test_golden_fixtures", "test_gpu_parity", "test_gpu_batch",
                 "test_gpu_serve", "test_cli", "test_gpu_lcp", "test_gpu_safile", "test_gpu_bwt", "test_gpu_gsa",
-                "test_gpu_batch_autotune", "test_gpu_timeout"]
+                "test_gpu_batch_autotune", "test_gpu_timeout", "test_gpu_fullsize"]
 
 
 def pytest_collection_modifyitems(config, items):
