@@ -38,7 +38,7 @@ sys.path.insert(0, ROOT)
 
 GiB = float(1 << 30)
 DEFAULT_WORKLOAD = "cfg2_dc39_markov_dna_1GiB"
-RADIX_KERNEL = "k_onesweep_st"
+RADIX_KERNEL = "k_onesweep"
 
 
 def _dist():

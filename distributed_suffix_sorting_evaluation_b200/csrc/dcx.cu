@@ -425,7 +425,6 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         }
     }
     if (run.empty()) return 0;
-    constexpr int ITEMS = ONESWEEP_ITEMS;
     constexpr int TILE = ONESWEEP_TILE;
     const uint64_t tiles = div_up(count, TILE);
     if (tiles > c.lookback_tiles) {
@@ -445,13 +444,20 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
     cudaEventCreate(&e1);
     cudaEventRecord(e0, c.stream);
     int cur = 0;
-    const size_t smem = onesweep_st_smem(kw);
-    DCX_CUDA(cudaFuncSetAttribute(k_onesweep_st<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)onesweep_st_smem(3)));
-    bool aligned16 = true;
+    const size_t smem = onesweep_smem(kw);
+    static bool attr_set = false;  // the attribute is per function, the same for every context
+    if (!attr_set) {
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(1)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(2)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(3)));
+        attr_set = true;
+    }
+    // full tiles are staged with 16-byte copies: every buffer comes from the
+    // context's allocator, which aligns to 256 bytes
     for (int b = 0; b < 2; b++) {
-        for (uint32_t w = 0; w < kw; w++) aligned16 &= ((uintptr_t)s.k[b][w] & 15) == 0;
-        aligned16 &= ((uintptr_t)s.v[b] & 15) == 0;
+        for (uint32_t w = 0; w < kw; w++)
+            if ((uintptr_t)s.k[b][w] & 15) throw Error(DCX_ERR_INTERNAL, "radix key buffer not 16-byte aligned");
+        if ((uintptr_t)s.v[b] & 15) throw Error(DCX_ERR_INTERNAL, "radix value buffer not 16-byte aligned");
     }
     for (size_t i = 0; i < run.size(); i++) {
         if (++c.epoch >= (1u << 30)) {
@@ -476,7 +482,9 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         a.spin_limit = c.opt.spin_limit;
         a.hold_tile = c.opt.lookback_hold_tile;
         a.gave_up = c.d_err + 1;
-        k_onesweep_st<ITEMS><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a, aligned16);
+        if (kw == 1) k_onesweep<1><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+        else if (kw == 2) k_onesweep<2><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+        else k_onesweep<3><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
         DCX_CHECK_LAUNCH();
         cur ^= 1;
     }

@@ -3,7 +3,7 @@
 // distributed comparison sorts (lightweight_dcx/src/sorters/sorting_wrapper.hpp:57-94,
 // sample_sort.hpp:36-171) for every sort of the DCX pipeline.
 //
-// One kernel per 8-bit digit (k_onesweep_st):
+// One kernel per 8-bit digit (k_onesweep<KW>, 4096-element tiles, three CTAs per SM):
 //   * tiles are claimed in order through an atomic counter;
 //   * the words the pass does not rank on (other key words, the value) are
 //     prefetched into shared memory with cp.async as soon as the tile is
@@ -14,7 +14,9 @@
 //     look-back; every wait is bounded and, when exhausted, sets an error bit
 //     and lets the CTA finish;
 //   * every array is exchanged through shared memory into digit order so that
-//     global writes of one digit run are contiguous.
+//     global writes of one digit run are contiguous;
+//   * full tiles (all but the last) run a copy of the tile code without
+//     per-item bounds tests.
 // Global digit offsets for every pass come from one up-front histogram that the
 // key producer fuses into its own pass (no extra read of the keys).
 #pragma once
@@ -86,54 +88,47 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-constexpr int ONESWEEP_ITEMS = 12;  // 3072-element tiles
+constexpr int ONESWEEP_ITEMS = 16;  // 4096-element tiles
 constexpr int ONESWEEP_TILE = SORT_THREADS * ONESWEEP_ITEMS;
+constexpr int ONESWEEP_MIN_CTAS = 3;  // register budget: three 256-thread CTAs per SM
 
-// Dynamic shared memory of k_onesweep_st: the exchange buffer plus one staging
-// buffer per carried array (kw - 1 other key words and the value).
-__host__ __device__ constexpr size_t onesweep_st_smem(uint32_t kw) {
+// Dynamic shared memory of k_onesweep<KW>: the exchange buffer plus one staging
+// buffer per carried array (KW - 1 other key words and the value).
+__host__ __device__ constexpr size_t onesweep_smem(uint32_t kw) {
     return sizeof(uint32_t) * (size_t)ONESWEEP_TILE * (1 + kw);
 }
 
-// One LSD pass.  `aligned16`: every array base is 16-byte aligned, so full
-// tiles are staged with 16-byte copies (the last, partial tile always uses
-// 4-byte copies, which never read past the array end).
-template <int ITEMS>
-__global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bool aligned16) {
+// Shared state of one CTA of k_onesweep (static shared memory).
+struct OnesweepShared {
+    uint32_t warp_hist[SORT_THREADS / 32][RADIX];  // per-warp digit counts, then running bases
+    uint32_t tile_excl[RADIX];                     // exclusive digit offsets inside the tile
+    uint32_t gbase[RADIX];                         // global destination of the tile's digit runs
+    uint32_t scan[SORT_THREADS / 32 + 1];
+    uint32_t tile;
+    uint32_t gave_up;
+};
+
+// One tile of one LSD pass over KW key words and a value.  FULL: the tile holds
+// TILE valid elements (every tile but the last), which drops every per-item
+// bounds test; the last tile marks missing elements with digit RADIX.
+template <int KW, int ITEMS, bool FULL>
+__device__ __forceinline__ void onesweep_tile(const SortPassArgs& a, OnesweepShared& sm, uint32_t* s_exch,
+                                              uint32_t* s_stage, uint64_t tile, uint32_t tile_valid) {
     constexpr int THREADS = SORT_THREADS;
     constexpr int WARPS = THREADS / 32;
     constexpr int TILE = THREADS * ITEMS;
     constexpr int LB_WINDOW = 4;
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warp_hist[WARPS][RADIX];
-    __shared__ uint32_t s_tile_excl[RADIX];
-    __shared__ uint32_t s_gbase[RADIX];
-    __shared__ uint32_t s_scan[THREADS / 32 + 1];
-    __shared__ uint32_t s_gave_up;
-    extern __shared__ __align__(16) uint32_t s_dyn[];
-    uint32_t* s_exch = s_dyn;           // [TILE]
-    uint32_t* s_stage = s_dyn + TILE;   // [kw][TILE]: carried arrays in tile order
-
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        s_tile = atomicAdd(a.tile_counter, 1u);
-        s_gave_up = 0;
-    }
-    for (int i = tid; i < WARPS * RADIX; i += THREADS) (&s_warp_hist[0][0])[i] = 0;
-    __syncthreads();
-    const uint64_t tile = s_tile;
     const uint64_t tile_base = tile * TILE;
-    const uint64_t remain = a.n - tile_base;
-    const uint32_t tile_valid = remain < (uint64_t)TILE ? (uint32_t)remain : (uint32_t)TILE;
     const int wd = a.shift >> 5, sh = a.shift & 31;
-    const int kw = (int)a.kw;
 
     // 0. prefetch the carried arrays (slot s: key word s < wd ? s : s + 1, the value last)
-    for (int s = 0; s < kw; s++) {
+#pragma unroll
+    for (int s = 0; s < KW; s++) {
         const int w = s < wd ? s : s + 1;
-        const uint32_t* src = (w < kw ? a.keys_in[w] : a.vals_in) + tile_base;
+        const uint32_t* src = (w < KW ? a.keys_in[w] : a.vals_in) + tile_base;
         uint32_t* dst = s_stage + s * TILE;
-        if (aligned16 && tile_valid == (uint32_t)TILE) {
+        if (FULL) {
 #pragma unroll
             for (int i = 0; i < TILE / 4 / THREADS; i++) {
                 const int c = (i * THREADS + tid) * 4;
@@ -147,19 +142,18 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
 
     // 1. digit word (warp-blocked: item `it` of lane l in warp w is tile element
     //    w*32*ITEMS + it*32 + l) and early counts per warp
-    uint32_t kword[ITEMS];
-    uint32_t dig[ITEMS];
+    uint32_t kword[ITEMS], dig[ITEMS], pos[ITEMS];
     const uint32_t* kin = a.keys_in[wd] + tile_base;
 #pragma unroll
     for (int it = 0; it < ITEMS; it++) {
         const uint32_t e = warp * 32 * ITEMS + it * 32 + lane;
-        kword[it] = e < tile_valid ? __ldg(kin + e) : 0u;
+        kword[it] = (FULL || e < tile_valid) ? __ldg(kin + e) : 0u;
     }
 #pragma unroll
     for (int it = 0; it < ITEMS; it++) {
         const uint32_t e = warp * 32 * ITEMS + it * 32 + lane;
-        dig[it] = e < tile_valid ? (kword[it] >> sh) & (RADIX - 1) : RADIX;
-        if (dig[it] < RADIX) atomicAdd(&s_warp_hist[warp][dig[it]], 1u);
+        dig[it] = (FULL || e < tile_valid) ? (kword[it] >> sh) & (RADIX - 1) : RADIX;
+        if (FULL || dig[it] < RADIX) atomicAdd(&sm.warp_hist[warp][dig[it]], 1u);
     }
     __syncthreads();
     uint32_t count = 0;
@@ -167,28 +161,26 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
         const int d = tid;
 #pragma unroll
         for (int w = 0; w < WARPS; w++) {
-            const uint32_t t = s_warp_hist[w][d];
-            s_warp_hist[w][d] = count;  // exclusive prefix over warps: the warp's running base
+            const uint32_t t = sm.warp_hist[w][d];
+            sm.warp_hist[w][d] = count;  // exclusive prefix over warps: the warp's running base
             count += t;
         }
         if (tile != a.hold_tile)
             st_relaxed(a.lookback + tile * RADIX + d, lb_pack(a.epoch, tile == 0 ? 2u : 1u, count));
         uint32_t total;
-        s_tile_excl[d] = block_excl_scan<THREADS>(count, s_scan, total);
+        sm.tile_excl[d] = block_excl_scan<THREADS>(count, sm.scan, total);
     }
     // 2. stable rank inside the warp, positions in the sorted tile
-    uint32_t pos[ITEMS];
-    const bool full = tile_valid == (uint32_t)TILE;
 #pragma unroll
     for (int it = 0; it < ITEMS; it++) {
         const uint32_t d = dig[it];
-        const uint32_t peers = full ? warp_digit_peers<false>(d) : warp_digit_peers<true>(d);
+        const uint32_t peers = warp_digit_peers<!FULL>(d);
         const uint32_t before = __popc(peers & lanemask_lt());
         uint32_t base = 0;
-        if (d < RADIX) base = s_warp_hist[warp][d];
+        if (FULL || d < RADIX) base = sm.warp_hist[warp][d];
         pos[it] = base + before;
         __syncwarp();
-        if (d < RADIX && before == 0) s_warp_hist[warp][d] = base + __popc(peers);
+        if ((FULL || d < RADIX) && before == 0) sm.warp_hist[warp][d] = base + __popc(peers);
         __syncwarp();
     }
     // 3. decoupled look-back for digit tid (bounded)
@@ -219,7 +211,7 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
                 if (k == 0) {
                     if (++spins > a.spin_limit) {
                         atomicOr(a.err, DEV_ERR_TIMEOUT);
-                        s_gave_up = 1;
+                        sm.gave_up = 1;
                         break;
                     }
                     if (spins > 32) __nanosleep(32);
@@ -227,27 +219,27 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
             }
             if (tile != a.hold_tile) st_relaxed(a.lookback + tile * RADIX + d, lb_pack(a.epoch, 2u, excl + count));
         }
-        s_gbase[d] = a.digit_base[d] + excl - s_tile_excl[d];
+        sm.gbase[d] = a.digit_base[d] + excl - sm.tile_excl[d];
     }
     __syncthreads();
-    if (tid == 0 && s_gave_up) atomicAdd(a.gave_up, 1u);
+    if (tid == 0 && sm.gave_up && a.gave_up) atomicAdd(a.gave_up, 1u);
 #pragma unroll
     for (int it = 0; it < ITEMS; it++)
-        if (dig[it] < RADIX) pos[it] += s_tile_excl[dig[it]];
+        if (FULL || dig[it] < RADIX) pos[it] += sm.tile_excl[dig[it]];
 
     // 4. digit word: exchange, destinations, store
     uint32_t dst[ITEMS];
 #pragma unroll
     for (int it = 0; it < ITEMS; it++)
-        if (dig[it] < RADIX) s_exch[pos[it]] = kword[it];
+        if (FULL || dig[it] < RADIX) s_exch[pos[it]] = kword[it];
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < ITEMS; it++) {
         const uint32_t j = it * THREADS + tid;
         dst[it] = 0xffffffffu;
-        if (j < tile_valid) {
+        if (FULL || j < tile_valid) {
             const uint32_t w = s_exch[j];
-            const uint32_t d = s_gbase[(w >> sh) & (RADIX - 1)] + j;
+            const uint32_t d = sm.gbase[(w >> sh) & (RADIX - 1)] + j;
             if (d < a.n) {
                 dst[it] = d;
                 a.keys_out[wd][d] = w;
@@ -258,21 +250,46 @@ __global__ __launch_bounds__(SORT_THREADS) void k_onesweep_st(SortPassArgs a, bo
     }
     // 5. carried arrays from the staging buffers, through the same exchange
     cp_async_wait_all();
-    for (int s = 0; s < kw; s++) {
+#pragma unroll
+    for (int s = 0; s < KW; s++) {
         const int w = s < wd ? s : s + 1;
-        uint32_t* out = w < kw ? a.keys_out[w] : a.vals_out;
+        uint32_t* out = w < KW ? a.keys_out[w] : a.vals_out;
         const uint32_t* stg = s_stage + s * TILE;
         __syncthreads();  // s_exch free, every thread's staged copies complete
 #pragma unroll
         for (int it = 0; it < ITEMS; it++)
-            if (dig[it] < RADIX) s_exch[pos[it]] = stg[warp * 32 * ITEMS + it * 32 + lane];
+            if (FULL || dig[it] < RADIX) s_exch[pos[it]] = stg[warp * 32 * ITEMS + it * 32 + lane];
         __syncthreads();
 #pragma unroll
         for (int it = 0; it < ITEMS; it++) {
             const uint32_t j = it * THREADS + tid;
-            if (j < tile_valid && dst[it] != 0xffffffffu) out[dst[it]] = s_exch[j];
+            if ((FULL || j < tile_valid) && dst[it] != 0xffffffffu) out[dst[it]] = s_exch[j];
         }
     }
+}
+
+// One LSD pass over KW key words (1..3) carrying one value.  Every array base
+// must be 16-byte aligned (full tiles are staged with 16-byte copies; the last,
+// partial tile uses 4-byte copies, which never read past the array end).
+template <int KW>
+__global__ __launch_bounds__(SORT_THREADS, ONESWEEP_MIN_CTAS) void k_onesweep(SortPassArgs a) {
+    constexpr int TILE = ONESWEEP_TILE;
+    __shared__ OnesweepShared sm;
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        sm.tile = atomicAdd(a.tile_counter, 1u);
+        sm.gave_up = 0;
+    }
+    for (int i = tid; i < (SORT_THREADS / 32) * RADIX; i += SORT_THREADS) (&sm.warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const uint64_t tile = sm.tile;
+    const uint64_t remain = a.n - tile * TILE;
+    const uint32_t tile_valid = remain < (uint64_t)TILE ? (uint32_t)remain : (uint32_t)TILE;
+    if (tile_valid == (uint32_t)TILE)
+        onesweep_tile<KW, ONESWEEP_ITEMS, true>(a, sm, s_dyn, s_dyn + TILE, tile, tile_valid);
+    else
+        onesweep_tile<KW, ONESWEEP_ITEMS, false>(a, sm, s_dyn, s_dyn + TILE, tile, tile_valid);
 }
 
 // Histogram of every 8-bit digit of keys already in memory (4*kw passes), for
