@@ -55,7 +55,7 @@ EXPORTED = (
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
     "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
     "dcx_build_gsa", "dcx_set_batch_dc_table", "dcx_get_batch_dc_table", "dcx_autotune_batch",
-    "dcx_write_sa_file", "dcx_read_sa_file", "dcx_check_sa_file", "dcx_bwt",
+    "dcx_write_sa_file", "dcx_read_sa_file", "dcx_check_sa_file", "dcx_bwt", "dcx_sort_u32", "dcx_build_sa_u32",
 )
 
 # serving request states (dcx_serve_poll)
@@ -146,6 +146,8 @@ def load_library(path: str | None = None):
     lib.dcx_write_sa_file.argtypes = [vp, ctypes.c_char_p, vp, u64, i32, u64]
     lib.dcx_read_sa_file.argtypes = [vp, ctypes.c_char_p, vp, u64, i32, u64]
     lib.dcx_check_sa_file.argtypes = [vp, vp, u64, ctypes.c_char_p, i32, u32, ctypes.POINTER(i32)]
+    lib.dcx_sort_u32.argtypes = [vp, vp, u32, vp, u64]
+    lib.dcx_build_sa_u32.argtypes = [vp, vp, u64, u64, i32, i32, vp]
     _lib = lib
     return lib
 
@@ -406,6 +408,17 @@ class Context:
         _check(self.lib.dcx_check_sa(self.h, ctypes.c_void_p(text_ptr), n, ctypes.c_void_p(sa_ptr), sa_width,
                                      DCX_DEVICE_PTRS, ctypes.byref(ok)))
         return bool(ok.value)
+
+    def sort_u32_device(self, key_ptrs, val_ptr: int, n: int):
+        """Stable in-place sort of n (key words, value) pairs in device memory,
+        key_ptrs[-1] the most significant uint32 word (1 to 3 words)."""
+        arr = (ctypes.c_void_p * len(key_ptrs))(*[ctypes.c_void_p(p) for p in key_ptrs])
+        _check(self.lib.dcx_sort_u32(self.h, arr, len(key_ptrs), ctypes.c_void_p(val_ptr), n))
+
+    def build_sa_u32_device(self, text_ptr: int, n: int, sigma: int, sa_ptr: int, dc: int = 3, sa_width: int = 32):
+        """SA of a device string of n uint32 symbols in [1, sigma] into a device buffer."""
+        _check(self.lib.dcx_build_sa_u32(self.h, ctypes.c_void_p(text_ptr), n, sigma, dc, sa_width,
+                                         ctypes.c_void_p(sa_ptr)))
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""

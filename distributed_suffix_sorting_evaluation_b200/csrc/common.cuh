@@ -99,8 +99,8 @@ __device__ __forceinline__ T block_excl_scan(T v, T* smem, T& total) {
 }
 
 // ---------------------------------------------------------------------------
-// Device-wide exclusive scan in three phases (tile reduce, scan of tile sums,
-// tile rescan).  Op supplies   T load(uint64_t i)   and
+// Device-wide exclusive scan in three phases (chunk reduce, scan of chunk sums,
+// chunk rescan).  Op supplies   T load(uint64_t i)   and
 //   void store(uint64_t i, T exclusive_prefix, T value)   for i < n.
 // No inter-CTA waits, so nothing can spin.
 // ---------------------------------------------------------------------------
@@ -117,36 +117,45 @@ struct ScanVec : std::false_type {};
 template <typename Op>
 struct ScanVec<Op, std::void_t<decltype(&Op::load16)>> : std::true_type {};
 
-// Loads are warp-striped: lane l of warp w reads element w*32*ITEMS + it*32 + l
-// of the tile in iteration it, so every load instruction is coalesced.
+// Every CTA owns a contiguous run of `tpc` tiles (chunk) and walks it in
+// order, so a scan of a billion elements runs as a few hundred CTAs rather
+// than hundreds of thousands of one-tile CTAs.
+//
+// Reduce phase: loads are warp-striped (lane l of warp w reads element
+// w*32*ITEMS + it*32 + l of the tile in iteration it), so every load
+// instruction is coalesced; one sum per chunk.
 template <typename T, typename Op>
-__global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(Op op, uint64_t n, T* tile_sums) {
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(Op op, uint64_t n, T* chunk_sums, uint64_t tpc) {
     __shared__ T sm[SCAN_THREADS / 32 + 1];
+    const uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    const uint64_t t0 = (uint64_t)blockIdx.x * tpc;
+    const uint64_t t1 = t0 + tpc < ntiles ? t0 + tpc : ntiles;
     T acc = T(0);
-    if constexpr (ScanVec<Op>::value) {
-        static_assert(SCAN_ITEMS == 16, "load16 covers a thread's items");
-        const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
-        if (base < n) {
-            T v[16];
-            op.load16(base, n, v);
+    for (uint64_t tile = t0; tile < t1; tile++) {
+        if constexpr (ScanVec<Op>::value) {
+            static_assert(SCAN_ITEMS == 16, "load16 covers a thread's items");
+            const uint64_t base = tile * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+            if (base < n) {
+                T v[16];
+                op.load16(base, n, v);
 #pragma unroll
-            for (int it = 0; it < 16; it++) acc += v[it];
-        }
-    } else {
-        const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)(threadIdx.x >> 5) * 32 * SCAN_ITEMS +
-                              (threadIdx.x & 31);
+                for (int it = 0; it < 16; it++) acc += v[it];
+            }
+        } else {
+            const uint64_t base = tile * SCAN_TILE + (uint64_t)(threadIdx.x >> 5) * 32 * SCAN_ITEMS + (threadIdx.x & 31);
 #pragma unroll
-        for (int it = 0; it < SCAN_ITEMS; it++) {
-            const uint64_t i = base + (uint64_t)it * 32;
-            if (i < n) acc += op.load(i);
+            for (int it = 0; it < SCAN_ITEMS; it++) {
+                const uint64_t i = base + (uint64_t)it * 32;
+                if (i < n) acc += op.load(i);
+            }
         }
     }
     T total;
     block_excl_scan<SCAN_THREADS>(acc, sm, total);
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+    if (threadIdx.x == 0) chunk_sums[blockIdx.x] = total;
 }
 
-// Single-CTA exclusive scan of the tile sums (in place); also writes the grand total.
+// Single-CTA exclusive scan of the chunk sums (in place); also writes the grand total.
 template <typename T>
 __global__ __launch_bounds__(1024) void k_scan_tile_sums(T* sums, uint64_t count, T* grand_total) {
     __shared__ T sm[1024 / 32 + 1];
@@ -162,39 +171,47 @@ __global__ __launch_bounds__(1024) void k_scan_tile_sums(T* sums, uint64_t count
     if (threadIdx.x == 0 && grand_total) *grand_total = carry;
 }
 
-// Apply phase: thread t owns SCAN_ITEMS consecutive elements of the tile (each
-// thread's loads walk one contiguous 16-element run, fully used through L1).
+// Apply phase: thread t owns SCAN_ITEMS consecutive elements of each tile
+// (each thread's loads walk one contiguous 16-element run, fully used through
+// L1); the chunk's running prefix carries from tile to tile.
 template <typename T, typename Op>
-__global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(Op op, uint64_t n, const T* tile_prefix) {
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(Op op, uint64_t n, const T* chunk_prefix, uint64_t tpc) {
     __shared__ T sm[SCAN_THREADS / 32 + 1];
-    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
-    T vals[SCAN_ITEMS];
-    T acc = T(0);
-    if constexpr (ScanVec<Op>::value) {
-        if (base < n) {
-            op.load16(base, n, vals);
+    const uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    const uint64_t t0 = (uint64_t)blockIdx.x * tpc;
+    const uint64_t t1 = t0 + tpc < ntiles ? t0 + tpc : ntiles;
+    T carry = chunk_prefix[blockIdx.x];
+    for (uint64_t tile = t0; tile < t1; tile++) {
+        const uint64_t base = tile * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+        T vals[SCAN_ITEMS];
+        T acc = T(0);
+        if constexpr (ScanVec<Op>::value) {
+            if (base < n) {
+                op.load16(base, n, vals);
+            } else {
+#pragma unroll
+                for (int it = 0; it < SCAN_ITEMS; it++) vals[it] = T(0);
+            }
+#pragma unroll
+            for (int it = 0; it < SCAN_ITEMS; it++) acc += vals[it];
         } else {
 #pragma unroll
-            for (int it = 0; it < SCAN_ITEMS; it++) vals[it] = T(0);
+            for (int it = 0; it < SCAN_ITEMS; it++) {
+                const uint64_t i = base + it;
+                vals[it] = i < n ? op.load(i) : T(0);
+                acc += vals[it];
+            }
         }
-#pragma unroll
-        for (int it = 0; it < SCAN_ITEMS; it++) acc += vals[it];
-    } else {
+        T total;
+        const T ex = block_excl_scan<SCAN_THREADS>(acc, sm, total);
+        T run = carry + ex;
 #pragma unroll
         for (int it = 0; it < SCAN_ITEMS; it++) {
             const uint64_t i = base + it;
-            vals[it] = i < n ? op.load(i) : T(0);
-            acc += vals[it];
+            if (i < n) op.store(i, run, vals[it]);
+            run += vals[it];
         }
-    }
-    T total;
-    const T ex = block_excl_scan<SCAN_THREADS>(acc, sm, total);
-    T run = tile_prefix[blockIdx.x] + ex;
-#pragma unroll
-    for (int it = 0; it < SCAN_ITEMS; it++) {
-        const uint64_t i = base + it;
-        if (i < n) op.store(i, run, vals[it]);
-        run += vals[it];
+        carry += total;
     }
 }
 

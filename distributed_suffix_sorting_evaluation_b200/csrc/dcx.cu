@@ -357,10 +357,12 @@ template <typename T, typename Op>
 static T device_scan(Ctx& c, const Op& op, uint64_t n) {
     if (n == 0) return T(0);
     const uint64_t tiles = div_up(n, SCAN_TILE);
-    DBuf<T> sums(&c, tiles + 1);
-    k_scan_reduce<T, Op><<<(unsigned)tiles, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get());
-    k_scan_tile_sums<T><<<1, 1024, 0, c.stream>>>(sums.get(), tiles, sums.get() + tiles);
-    k_scan_apply<T, Op><<<(unsigned)tiles, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get());
+    const uint64_t tpc = div_up(tiles, 148 * 6);  // tiles per CTA: about six CTAs per SM
+    const uint64_t chunks = div_up(tiles, tpc);
+    DBuf<T> sums(&c, chunks + 1);
+    k_scan_reduce<T, Op><<<(unsigned)chunks, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get(), tpc);
+    k_scan_tile_sums<T><<<1, 1024, 0, c.stream>>>(sums.get(), chunks, sums.get() + chunks);
+    k_scan_apply<T, Op><<<(unsigned)chunks, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get(), tpc);
     DCX_CHECK_LAUNCH();
     c.launched(3);
     return d2h_scalar(c, sums.get() + tiles);
@@ -1108,11 +1110,40 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
     // sample records in sample text order (one random scatter)
     DBuf<uint64_t> srec(&c, slots);
     DCX_CUDA(cudaMemsetAsync(srec.get(), 0xff, slots * 8, c.stream));
-    k_scatter_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), s_seg.get(), name.get(), uniq.get(),
-                                                             dfl.get(), ls, srec.get());
-    DCX_CHECK_LAUNCH();
-    c.launched();
-    c.alg(m * 21);
+    if (slots <= (1u << 20)) {  // 8 MB of records: a direct scatter stays in L2
+        k_scatter_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s_pos.get(), s_seg.get(), name.get(), uniq.get(),
+                                                                 dfl.get(), ls, srec.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(m * 21);
+    } else {
+        // group the records by the second-highest byte of their slot first
+        uint32_t bits = 0;
+        while (bits < 32 && ((slots - 1) >> bits)) bits++;
+        const uint32_t byte = (bits + 7) / 8 >= 2 ? (bits + 7) / 8 - 2 : 0;
+        SortSpace s;
+        DBuf<uint32_t> rk[2][2], rv[2];
+        for (int b = 0; b < 2; b++) {
+            for (int w = 0; w < 2; w++) {
+                rk[b][w] = DBuf<uint32_t>(&c, m);
+                s.k[b][w] = rk[b][w].get();
+            }
+            rv[b] = DBuf<uint32_t>(&c, m);
+            s.v[b] = rv[b].get();
+        }
+        DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+        k_sample_records<<<grid_for(m, 256, 148 * 8), 256, 0, c.stream>>>(m, s_pos.get(), s_seg.get(), name.get(),
+                                                                          uniq.get(), dfl.get(), ls, s.k[0][0],
+                                                                          s.k[0][1], s.v[0], c.d_hist, byte);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(m * 21);
+        const int f = radix_sort(c, 2, m, s);
+        k_scatter_records<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s.k[f][0], s.k[f][1], s.v[f], srec.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(m * 20);
+    }
     s_pos.reset();
     s_seg.reset();
     uniq.reset();
@@ -1440,6 +1471,73 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
     cudaEventDestroy(e3);
+}
+
+// ---------------------------------------------------------------------------
+// Building blocks of the multi-GPU single-text build (distributed.py): a stable
+// device sort of (key words, value) pairs and the SA of a 32-bit string.
+// ---------------------------------------------------------------------------
+// Sorts n pairs in place by their kw little-endian uint32 key words (word kw-1
+// most significant), stable, with the onesweep passes of every other sort.
+static void sort_u32(Ctx& c, uint32_t* const* keys, uint32_t kw, uint32_t* vals, uint64_t n) {
+    if (kw < 1 || kw > 3) throw Error(DCX_ERR_ARG, "1 to 3 key words");
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "more than 2^32 - 2 pairs");
+    if (n <= 1) return;
+    if (!keys || !vals) throw Error(DCX_ERR_ARG, "null pointer");
+    for (uint32_t w = 0; w < kw; w++)
+        if (!keys[w] || ((uintptr_t)keys[w] & 15)) throw Error(DCX_ERR_ARG, "key arrays must be 16-byte aligned");
+    if ((uintptr_t)vals & 15) throw Error(DCX_ERR_ARG, "value array must be 16-byte aligned");
+    c.st = dcx_stats{};
+    c.peak = c.in_use;
+    SortSpace s;
+    DBuf<uint32_t> k1[3], v1(&c, n);
+    for (uint32_t w = 0; w < kw; w++) {
+        k1[w] = DBuf<uint32_t>(&c, n);
+        s.k[0][w] = keys[w];
+        s.k[1][w] = k1[w].get();
+    }
+    s.v[0] = vals;
+    s.v[1] = v1.get();
+    DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+    SortPassArgs ha{};
+    for (uint32_t w = 0; w < kw; w++) ha.keys_in[w] = keys[w];
+    ha.kw = kw;
+    ha.n = n;
+    k_digit_hist<<<grid_for(n, 256, 148 * 4), 256, 4 * kw * RADIX * 4, c.stream>>>(ha, c.d_hist);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    c.alg(n * 4 * kw);
+    const int f = radix_sort(c, kw, n, s);
+    if (f == 1) {
+        for (uint32_t w = 0; w < kw; w++)
+            DCX_CUDA(cudaMemcpyAsync(keys[w], k1[w].get(), n * 4, cudaMemcpyDeviceToDevice, c.stream));
+        DCX_CUDA(cudaMemcpyAsync(vals, v1.get(), n * 4, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    c.st.peak_bytes = c.peak;
+}
+
+// SA of a device string of n 32-bit symbols in [1, sigma] (the recursion
+// strings of the multi-GPU build): one DCX pipeline as for a recursion level.
+static void build_u32(Ctx& c, const uint32_t* text, uint64_t n, uint64_t sigma, int X, int width, void* sa_out) {
+    if (n >= 0xffffffffull) throw Error(DCX_ERR_ARG, "string longer than 2^32 - 2");
+    if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
+    if (sigma == 0 || sigma >= 0xffffffffull) throw Error(DCX_ERR_ARG, "alphabet bound must be in [1, 2^32 - 2]");
+    if (n && (!text || !sa_out)) throw Error(DCX_ERR_ARG, "null pointer");
+    get_dc(c, (uint32_t)X);
+    c.st = dcx_stats{};
+    c.peak = c.in_use;
+    if (n == 0) return;
+    DBuf<uint32_t> t(&c, n + 1);
+    DCX_CUDA(cudaMemcpyAsync(t.get(), text, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+    DCX_CUDA(cudaMemsetAsync(t.get() + n, 0, 4, c.stream));
+    Segs one;
+    one.start = {0, n + 1};
+    c.level0_entropy = 0;
+    level<uint32_t>(c, t.get(), one, sigma, (uint32_t)X, 1, false, sa_out, width);
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_error(c);
+    c.st.peak_bytes = c.peak;
 }
 
 // ---------------------------------------------------------------------------
@@ -2353,6 +2451,25 @@ int dcx_get_trace(dcx_ctx* x, uint64_t* m_out, uint32_t* names, uint8_t* unique,
         if (unique) memcpy(unique, x->c.trace_uniq.data(), m);
     }
     return DCX_OK;
+}
+
+int dcx_sort_u32(dcx_ctx* x, uint32_t* const* keys_dev, uint32_t kw, uint32_t* vals_dev, uint64_t n) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::sort_u32(x->c, keys_dev, kw, vals_dev, n);
+    });
+}
+
+int dcx_build_sa_u32(dcx_ctx* x, const uint32_t* text_dev, uint64_t n, uint64_t sigma, int dc, int sa_width,
+                     void* sa_out_dev) {
+    if (!x) return DCX_ERR_ARG;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(x->c.build_mu);
+        DCX_CUDA(cudaSetDevice(x->c.device));
+        dcx::build_u32(x->c, text_dev, n, sigma, dc, sa_width, sa_out_dev);
+    });
 }
 
 int dcx_build_sa_batch(dcx_ctx* x, const uint8_t* texts, const uint64_t* offsets, uint32_t num_texts,

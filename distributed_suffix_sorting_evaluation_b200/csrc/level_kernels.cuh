@@ -365,6 +365,39 @@ __global__ void k_scatter_samples(uint64_t m, const uint32_t* __restrict__ s_pos
     }
 }
 
+// The same records in two steps for large levels, so that no store is a lone
+// 8-byte write into a 32-byte sector: k_sample_records lays each sample out as
+// (slot, name, unique | j << 1) and histograms one byte of the slot; one radix
+// pass on that byte groups the samples by 1/256 of the slot range; then
+// k_scatter_records stores them in that order, so the stores of concurrent
+// CTAs land in a few megabytes that L2 fills completely before writing back.
+__global__ void k_sample_records(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ s_seg,
+                                 const uint32_t* __restrict__ name, const uint8_t* __restrict__ uniq,
+                                 const DcFlags* __restrict__ f, LevelSeg ls, uint32_t* __restrict__ slot_out,
+                                 uint32_t* __restrict__ name_out, uint32_t* __restrict__ hi_out,
+                                 uint32_t* __restrict__ hist, uint32_t byte) {
+    __shared__ uint32_t h[RADIX];
+    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const DcFlags& F = *f;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = (uint32_t)(ls.rbase[s_seg ? s_seg[j] : 0u] + slot_of_local(s_pos[j], F));
+        slot_out[j] = k;
+        name_out[j] = name[j];
+        hi_out[j] = (uint32_t)uniq[j] | ((uint32_t)j << 1);
+        atomicAdd(&h[(k >> (8 * byte)) & (RADIX - 1)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < RADIX; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[byte * RADIX + i], h[i]);
+}
+
+__global__ void k_scatter_records(uint64_t m, const uint32_t* __restrict__ slot, const uint32_t* __restrict__ lo,
+                                  const uint32_t* __restrict__ hi, uint64_t* __restrict__ srec) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x)
+        srec[slot[j]] = (uint64_t)lo[j] | ((uint64_t)hi[j] << 32);
+}
+
 // Distinct names: the rank of every sample is its name (padding slots stay 0).
 __global__ void k_ranks_from_names(uint64_t slots, const uint64_t* __restrict__ srec, uint32_t* __restrict__ rank_text,
                                    uint32_t* trace_names, uint8_t* trace_uniq) {

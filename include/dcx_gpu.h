@@ -199,6 +199,25 @@ int dcx_get_stats(dcx_ctx* ctx, dcx_stats* out);
  * (slot = (i/X)*D + NEXT_RANK[i%X], pdcx/merge_samples.hpp:181-188). */
 int dcx_get_trace(dcx_ctx* ctx, uint64_t* m_out, uint32_t* names, uint8_t* unique, uint64_t capacity);
 
+/* ---- building blocks of the multi-GPU single-text build --------------------- */
+/* The reference distributes one text over MPI ranks and sorts with a
+ * distributed sample sort (lightweight_dcx/src/sorters/sample_sort.hpp:36-171,
+ * mpi/alltoall.hpp:106-137); distributed.py does the same over
+ * torch.distributed with these two device calls as its local steps.
+ * dcx_sort_u32 sorts n pairs in place, stable, by kw (1..3) little-endian
+ * uint32 key words (keys_dev[kw-1] most significant) carrying one uint32
+ * value: the onesweep radix passes of every sort in this library (the local
+ * sort that replaces ips4o in SortingWrapper::sort, sorters/sorting_wrapper.hpp:57-94).
+ * Every array is a device buffer, 16-byte aligned; n < 2^32 - 1. */
+int dcx_sort_u32(dcx_ctx* ctx, uint32_t* const* keys_dev, uint32_t kw, uint32_t* vals_dev, uint64_t n);
+/* Suffix array of a device string of n uint32 symbols, each in [1, sigma]
+ * (no 0: it marks the end), into the device buffer sa_out_dev (sa_width 32,
+ * 40 or 64): the recursive call on the names of the samples
+ * (PDCX::handle_recursive_call, pdcx/pdcx.hpp:146-180) when the recursion
+ * string is gathered onto one GPU.  dc as for dcx_build_sa. */
+int dcx_build_sa_u32(dcx_ctx* ctx, const uint32_t* text_dev, uint64_t n, uint64_t sigma, int dc, int sa_width,
+                     void* sa_out_dev);
+
 /* ---- batch ----------------------------------------------------------------- */
 /* Builds one SA per text.  texts is the concatenation, offsets[num_texts+1] the
  * text boundaries (offsets[0] = 0).  sa_out receives, per text, its SA with

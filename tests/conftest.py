@@ -24,7 +24,8 @@ def pytest_configure(config):
 # in a consumer then never hides the state of the build it consumes.
 _SUITE_ORDER = ["test_abi", "test_oracle", "test_golden_fixtures", "test_gpu_parity", "test_gpu_batch",
                 "test_gpu_serve", "test_cli", "test_gpu_lcp", "test_gpu_safile", "test_gpu_bwt", "test_gpu_gsa",
-                "test_gpu_batch_autotune", "test_gpu_timeout", "test_gpu_fullsize"]
+                "test_gpu_batch_autotune", "test_gpu_timeout", "test_distributed", "test_gpu_distributed",
+                "test_gpu_fullsize"]
 
 
 def pytest_collection_modifyitems(config, items):
