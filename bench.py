@@ -299,6 +299,102 @@ def gsa_sample_check(d_set, d_gsa, pairs: int, seed: int) -> str:
     return f"permutation + {pairs} sampled adjacent pairs in order"
 
 
+def run_split(args, world, rank, local):
+    """One text spread over all ranks (--split-text): rank r holds the block
+    T[r*n//N, (r+1)*n//N) and the ranks build the one suffix array together
+    with the distributed sample sort of distributed.py (NCCL exchanges; strong
+    scaling: the whole job builds one text).  value: text bytes / slowest
+    rank's device time of the whole collective build, block already on the
+    GPU.  e2e: the same with the block copied from pinned host memory and the
+    rank's SA slice copied back inside each step."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
+    from distributed_suffix_sorting_evaluation_b200 import distributed as Dd
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world == 1:  # one rank without torchrun: a local rendezvous
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", str(29500 + os.getpid() % 1000))
+    if not dist.is_initialized():
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev,
+                                world_size=world, rank=rank)
+    w = dict(W.WORKLOADS[args.workload])
+    if args.text_mib:
+        w["n"] = args.text_mib << 20
+    n = int(w["n"])
+    text = getattr(W, w["gen"])(n, seed=w["seed"])  # the same text on every rank
+    lo, hi = rank * n // world, (rank + 1) * n // world
+    h_block = torch.from_numpy(text[lo:hi].copy()).pin_memory()
+    d_block = h_block.to(dev)
+    ctx = Context(local)
+    ops = Dd.DeviceOps(ctx, dev)
+
+    def step(block):
+        return Dd.build_sa_distributed(block, n, dc=w["dc"], ops=ops)
+
+    for _ in range(args.warmup):
+        step(d_block)
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            loc = step(d_block)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+    clock = clocks.summary()
+    ms = max_over_ranks(ms, world, dev)
+    ms_step = ms / args.steps
+    verified = None
+    if args.verify:
+        full = Dd.gather_sa(loc)
+        if rank == 0:
+            ok = ctx.check_sa_device(torch.from_numpy(text).to(dev).data_ptr(), n,
+                                     full.to(torch.int64).contiguous().data_ptr(), 64)
+            verified = bool(ok)
+            if not ok:
+                raise SystemExit("the distributed suffix array failed the GPU check")
+        del full
+    # end to end: pinned block in, SA slice out
+    e2e_ms = []
+    for _ in range(max(1, min(args.steps, args.e2e_steps))):
+        dist.barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        sl = step(h_block.to(dev, non_blocking=True))
+        host_sa = sl.cpu()
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms.append(max_over_ranks(a.elapsed_time(b), world, dev))
+    ms_e2e = statistics.median(e2e_ms)
+    if rank == 0:
+        line = {
+            "metric": "SA build GiB/s", "value": round(n / GiB / (ms_step / 1000.0), 4), "unit": "GiB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
+            "data": W.DESCRIPTIONS[args.workload],
+            "config": {"workload": args.workload if not args.text_mib else f"{args.workload}@{args.text_mib}MiB",
+                       "text_bytes": n, "dc": w["dc"], "sa_width": 64,
+                       "l2_flush": "inputs larger than L2", "parallelism": f"split text over {world} ranks"},
+            "e2e": {"value": round(n / GiB / (ms_e2e / 1000.0), 4), "unit": "GiB/s",
+                    "h2d_bytes_per_step": int(hi - lo), "d2h_bytes_per_step": int(host_sa.numel() * 8),
+                    "statistic": "median step, max over ranks"},
+            "verified": verified, "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    dist.destroy_process_group()
+    return 0
+
+
 def run_gpu(args, world, rank, local):
     import torch
     from distributed_suffix_sorting_evaluation_b200 import Context, workloads as W
@@ -944,6 +1040,8 @@ def main():
     ap.add_argument("--batch-split", default="lpt", choices=["lpt", "replicas"],
                     help="how the batched workload is split over ranks under torchrun")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")
+    ap.add_argument("--split-text", action="store_true",
+                    help="build ONE text over all ranks with the distributed sample sort (strong scaling)")
     ap.add_argument("--verify", action=argparse.BooleanOptionalAction, default=True,
                     help="check the SA (batched: three SAs per chunk) on the GPU after the timed region")
     ap.add_argument("--serve-requests", type=int, default=20000, help="request pool of the serving workload")
@@ -965,6 +1063,8 @@ def main():
         return run_batch(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.split_text:
+        return run_split(args, world, rank, local)
     return run_gpu(args, world, rank, local)
 
 

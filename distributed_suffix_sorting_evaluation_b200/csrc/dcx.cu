@@ -365,7 +365,7 @@ static T device_scan(Ctx& c, const Op& op, uint64_t n) {
     k_scan_apply<T, Op><<<(unsigned)chunks, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get(), tpc);
     DCX_CHECK_LAUNCH();
     c.launched(3);
-    return d2h_scalar(c, sums.get() + tiles);
+    return d2h_scalar(c, sums.get() + chunks);  // the grand total k_scan_tile_sums wrote
 }
 
 static const DcHost& get_dc(Ctx& c, uint32_t X) {
