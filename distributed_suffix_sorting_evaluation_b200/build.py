@@ -25,7 +25,7 @@ HOST_CXX = "/usr/bin/g++"
 
 SOURCES = ["dcx.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "radix.cuh", "keys.cuh", "segsort.cuh", "small_sa.cuh", "level_kernels.cuh", "lcp.cuh",
-           "bwt.cuh", "gsa.cuh", "serve.cuh"]
+           "lcp_scatter.cuh", "bwt.cuh", "gsa.cuh", "serve.cuh"]
 
 
 def _nvcc() -> str:

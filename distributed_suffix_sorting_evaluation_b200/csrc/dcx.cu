@@ -37,6 +37,7 @@
 #include "segsort.cuh"
 #include "small_sa.cuh"
 #include "lcp.cuh"
+#include "lcp_scatter.cuh"
 #include "bwt.cuh"
 #include "gsa.cuh"
 
@@ -608,13 +609,20 @@ static void refine_small_w(Ctx& c, const CharT* text, SegView sv, const uint32_t
         DCX_CHECK_LAUNCH();
         c.launched();
     }
-    const uint64_t g0 = tg.off[1], ng = tg.off[5] - g0;
-    if (ng) {
-        k_refine_warp<W, CharT><<<grid_for(ng * 32, 256, 148 * 16), 256, 0, c.stream>>>(
+    // classes 1..4 (3-4, 5-8, 9-16, 17-32 elements): 4, 8, 16 or 32 lanes per group
+    auto sub = [&](int cls, auto lanes) {
+        constexpr int LN = decltype(lanes)::value;
+        const uint64_t g0 = tg.off[cls], ng = tg.counts[cls];
+        if (!ng) return;
+        k_refine_warp<W, LN, CharT><<<grid_for(ng * LN, 256, 148 * 16), 256, 0, c.stream>>>(
             text, sv, segw, tg.gstart.get() + g0, tg.gsize.get() + g0, ng, sa, head, plan);
         DCX_CHECK_LAUNCH();
         c.launched();
-    }
+    };
+    sub(1, std::integral_constant<int, 4>{});
+    sub(2, std::integral_constant<int, 8>{});
+    sub(3, std::integral_constant<int, 16>{});
+    sub(4, std::integral_constant<int, 32>{});
 }
 
 template <int C, int T, typename CharT>
@@ -1921,6 +1929,40 @@ static bool check_sa_file(Ctx& c, const uint8_t* text, uint64_t n, const char* p
     return check_one(c, dtext, n, dsa.get(), width, DCX_DEVICE_PTRS);
 }
 
+// phi[SA[k]] = SA[k-1]: a direct scatter while phi fits L2 (16 MB), else the
+// two-step form (records, one radix pass on the second-highest byte of SA[k],
+// an L2-local scatter).
+static void build_phi(Ctx& c, const uint32_t* sa32, uint64_t n, uint32_t* phi) {
+    if (n <= (1u << 22)) {
+        k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32, n, phi);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(n * 12);
+        return;
+    }
+    uint32_t bits = 0;
+    while (bits < 32 && ((n - 1) >> bits)) bits++;
+    const uint32_t byte = (bits + 7) / 8 >= 2 ? (bits + 7) / 8 - 2 : 0;
+    SortSpace s;
+    DBuf<uint32_t> pk[2], pv[2];
+    for (int b = 0; b < 2; b++) {
+        pk[b] = DBuf<uint32_t>(&c, n);
+        pv[b] = DBuf<uint32_t>(&c, n);
+        s.k[b][0] = pk[b].get();
+        s.v[b] = pv[b].get();
+    }
+    DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+    k_phi_records<<<grid_for(n, 256, 148 * 8), 256, 0, c.stream>>>(sa32, n, s.k[0][0], s.v[0], c.d_hist, byte);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    c.alg(n * 16);
+    const int f = radix_sort(c, 1, n, s);
+    k_phi_scatter<<<grid_for(n, 256), 256, 0, c.stream>>>(s.k[f][0], s.v[f], n, phi);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    c.alg(n * 12);
+}
+
 // LCP (or PLCP with DCX_LCP_PERMUTED) of a text and its SA; lcp_width 32 or 64.
 static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, int sa_width, void* out,
                       int lcp_width, uint32_t flags) {
@@ -1944,8 +1986,9 @@ static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     }
     DBuf<uint32_t> phi(&c, n), sa32(&c, n), plcp(&c, n);
     k_sa_to_u32<<<grid_for(div_up(n, 4), 256), 256, 0, c.stream>>>(dsa, sa_width, n, sa32.get());
-    k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, phi.get());
     DCX_CHECK_LAUNCH();
+    c.launched();
+    build_phi(c, sa32.get(), n, phi.get());
     sa_in.reset();
     if (flags & DCX_LCP_GSA) {
         // a generalized SA: separators (0 bytes) are distinct symbols, no match runs through one
@@ -1969,7 +2012,7 @@ static void build_lcp(Ctx& c, const uint8_t* text, uint64_t n, const void* sa, i
     k_lcp_gather<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), plcp.get(), n, dout, lcp_width,
                                                         (flags & DCX_LCP_PERMUTED) != 0);
     DCX_CHECK_LAUNCH();
-    c.launched(4);
+    c.launched(2);
     if (!dev) DCX_CUDA(cudaMemcpyAsync(out, dout, n * lb, cudaMemcpyDeviceToHost, c.stream));
     DCX_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -2082,7 +2125,7 @@ static void build_gsa(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         DBuf<uint32_t> zb(&c, n), sep(&c, n / 2 + 1);  // no empty string: at most n/2 separators
         device_scan<uint32_t>(c, OpSeparators{t.get(), zb.get(), sep.get()}, n);
         DBuf<uint32_t> phi(&c, n), plcp(&c, n);
-        k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, phi.get());
+        build_phi(c, sa32.get(), n, phi.get());
         k_plcp_to_separator<<<grid_for(div_up(n, LCP_RUN), 128, 148 * 64), 128, 0, c.stream>>>(
             t.get(), n, phi.get(), zb.get(), sep.get(), plcp.get(), 1);
         DCX_CHECK_LAUNCH();
@@ -2090,7 +2133,7 @@ static void build_gsa(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
         k_gsa_heads<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32.get(), n, plcp.get(), zb.get(), sep.get(),
                                                             head.get());
         DCX_CHECK_LAUNCH();
-        c.launched(4);
+        c.launched(2);
     }
     // runs re-sorted by (run number, position)
     {

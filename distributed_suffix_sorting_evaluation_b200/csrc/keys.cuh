@@ -474,27 +474,37 @@ __global__ __launch_bounds__(256) void k_refine_pair(const CharT* __restrict__ t
     }
 }
 
-// Groups of 3..32 elements: one warp per group, one element per lane, a
-// bitonic network over the lanes with shuffles.
-template <int W, typename CharT>
+// Groups of 3..LANES elements (LANES = 4, 8, 16 or 32): LANES lanes per group,
+// 32 / LANES groups per warp, one element per lane, a bitonic network over the
+// group's lanes with shuffles.
+template <int W, int LANES, typename CharT>
 __global__ __launch_bounds__(256) void k_refine_warp(const CharT* __restrict__ text, SegView sv,
                                                      const uint32_t* __restrict__ segw,
                                                      const uint32_t* __restrict__ gstart,
                                                      const uint32_t* __restrict__ gsize, uint64_t ngroups,
                                                      uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
                                                      RefineSegPlan plan) {
+    static_assert(LANES >= 2 && LANES <= 32 && (LANES & (LANES - 1)) == 0, "power-of-two lanes");
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += warps) {
-        const uint32_t start = gstart[g], size = gsize[g];
-        const uint64_t end = seg_end(sv, segw ? segw[start] : 0u);
-        bool valid = lane < size;
-        uint32_t p = valid ? sa[start + lane] : 0u;
+    const uint32_t l = lane % LANES;
+    const uint64_t slots = ((uint64_t)gridDim.x * blockDim.x) / LANES;
+    for (uint64_t g0 = ((uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) / LANES;
+         g0 < ngroups; g0 += slots) {
+        const uint64_t g = g0 + lane / LANES;  // every lane of the warp runs the network
+        uint32_t start = 0, size = 0;
+        uint64_t end = 0;
+        if (g < ngroups) {
+            start = gstart[g];
+            size = gsize[g];
+            end = seg_end(sv, segw ? segw[start] : 0u);
+        }
+        bool valid = l < size;
+        uint32_t p = valid ? sa[start + l] : 0u;
         uint64_t key[W];
 #pragma unroll
         for (int w = 0; w < W; w++) key[w] = valid ? window_value_t(text, (uint64_t)p + plan.off[w], end, plan.rp[w]) : 0ull;
 #pragma unroll
-        for (int k = 2; k <= 32; k <<= 1) {
+        for (int k = 2; k <= LANES; k <<= 1) {
 #pragma unroll
             for (int j = k >> 1; j > 0; j >>= 1) {
                 const bool ov = __shfl_xor_sync(0xffffffffu, valid, j);
@@ -509,8 +519,8 @@ __global__ __launch_bounds__(256) void k_refine_warp(const CharT* __restrict__ t
                     if (!c && ok[w] != key[w]) c = ok[w] < key[w] ? -1 : 1;
                 const bool o_less = ov && (!valid || c < 0);
                 const bool m_less = valid && (!ov || c > 0);
-                const bool up = (k == 32) || ((lane & k) == 0);
-                const bool lower = (lane & j) == 0;
+                const bool up = (k == LANES) || ((l & k) == 0);
+                const bool lower = (l & j) == 0;
                 if ((lower == up) ? o_less : m_less) {
                     valid = ov;
                     p = op;
@@ -521,10 +531,10 @@ __global__ __launch_bounds__(256) void k_refine_warp(const CharT* __restrict__ t
         }
         bool diff = false;
 #pragma unroll
-        for (int w = 0; w < W; w++) diff |= __shfl_up_sync(0xffffffffu, key[w], 1) != key[w];
+        for (int w = 0; w < W; w++) diff |= __shfl_up_sync(0xffffffffu, key[w], 1, LANES) != key[w];
         if (valid) {
-            sa[start + lane] = p;
-            if (lane > 0) head[start + lane] = diff;
+            sa[start + l] = p;
+            if (l > 0) head[start + l] = diff;
         }
     }
 }

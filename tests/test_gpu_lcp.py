@@ -48,3 +48,23 @@ def test_lcp_of_gpu_sa_device(ctx, oracle):
     torch.cuda.synchronize()
     _, lcp = oracle.libsais_lcp(t)
     assert np.array_equal(d_lcp.cpu().numpy().astype(np.int64), lcp)
+
+
+def test_lcp_long_text_two_step_phi(ctx, oracle):
+    """Texts past 2^22 characters build Phi in two steps (records, one radix pass
+    on the second-highest byte of SA[k], an L2-local scatter); the LCP and PLCP
+    must still equal libsais's, as must the generalized SA and its LCP of a set
+    that long."""
+    t = random_text(6_000_000, 4, seed=77)
+    t[3_000_000:3_500_000] = t[100_000:600_000]  # a long repeat
+    sa = oracle.libsais(t)
+    plcp, lcp = oracle.libsais_lcp(t, sa)
+    assert np.array_equal(ctx.build_lcp(t, sa), lcp.astype(np.uint64))
+    assert np.array_equal(ctx.build_lcp(t, sa, permuted=True), plcp.astype(np.uint64))
+    s = random_text(5_000_000, 3, seed=78)
+    s[(1 << 20) - 1::1 << 20] = 0  # strings of 1 MiB, each ended by a 0
+    s[-1] = 0
+    gsa = oracle.libsais_gsa(s)
+    assert np.array_equal(ctx.build_gsa(s, dc=39, sa_width=64), gsa.astype(np.uint64))
+    _, glcp = oracle.libsais_lcp_gsa(s, gsa)
+    assert np.array_equal(ctx.build_lcp(s, gsa, gsa=True), glcp.astype(np.uint64))
