@@ -35,6 +35,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# the seeded text generators run OpenMP loops; idle OpenMP workers must sleep,
+# not spin on the host cores the timed builds need for their kernel launches
+os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
 
 GiB = float(1 << 30)
 DEFAULT_WORKLOAD = "cfg2_dc39_markov_dna_1GiB"

@@ -78,7 +78,7 @@ class DcxStats(ctypes.Structure):
         ("sigma", ctypes.c_uint32), ("level0_samples", ctypes.c_uint64), ("level0_last_rank", ctypes.c_uint64),
         ("level0_recursion", ctypes.c_int), ("level0_reduction", ctypes.c_double),
         ("tie_groups", ctypes.c_uint64), ("tie_elements", ctypes.c_uint64),
-        ("lookback_gave_up", ctypes.c_uint64),
+        ("lookback_gave_up", ctypes.c_uint64), ("pool_growth_bytes", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

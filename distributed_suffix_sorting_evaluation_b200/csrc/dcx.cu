@@ -331,6 +331,16 @@ static int grid_for(uint64_t n, int threads, int max_blocks = 148 * 16) {
     return (int)std::min<uint64_t>(b, (uint64_t)max_blocks);
 }
 
+// Bytes the context's allocation pool holds from the device (reserved, used or
+// not); a build that has to grow it pays for mapping new memory.
+static uint64_t pool_reserved(Ctx& c) {
+    cudaMemPool_t p = c.pool;
+    if (!p && cudaDeviceGetDefaultMemPool(&p, c.device) != cudaSuccess) return 0;
+    uint64_t v = 0;
+    if (cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &v) != cudaSuccess) return 0;
+    return (uint64_t)v;
+}
+
 // Small device->host reads go through the context's pinned staging area.
 template <typename T>
 static T d2h_scalar(Ctx& c, const T* dptr) {
@@ -1147,7 +1157,9 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
         c.launched();
         c.alg(m * 21);
         const int f = radix_sort(c, 2, m, s);
-        k_scatter_records<<<grid_for(m, 256), 256, 0, c.stream>>>(m, s.k[f][0], s.k[f][1], s.v[f], srec.get());
+        // resident CTAs only: one front through the grouped records (see build_phi)
+        k_scatter_records<<<grid_for(m, 256, 148 * 8), 256, 0, c.stream>>>(m, s.k[f][0], s.k[f][1], s.v[f],
+                                                                           srec.get());
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(m * 20);
@@ -1364,6 +1376,7 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     const bool dev = flags & DCX_DEVICE_PTRS;
     const bool packing = !(flags & DCX_NO_PACKING);
     cudaEvent_t e0, e1, e2, e3;
+    const uint64_t pool0 = pool_reserved(c);
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventCreate(&e2);
@@ -1475,6 +1488,8 @@ static void build_one(Ctx& c, const uint8_t* text, uint64_t n, int X, int width,
     c.st.ms_phase0 = p0;
     c.st.ms_total = total;
     c.st.peak_bytes = c.peak;
+    const uint64_t pool1 = pool_reserved(c);
+    c.st.pool_growth_bytes = pool1 > pool0 ? pool1 - pool0 : 0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
@@ -1957,7 +1972,10 @@ static void build_phi(Ctx& c, const uint32_t* sa32, uint64_t n, uint32_t* phi) {
     c.launched();
     c.alg(n * 16);
     const int f = radix_sort(c, 1, n, s);
-    k_phi_scatter<<<grid_for(n, 256), 256, 0, c.stream>>>(s.k[f][0], s.v[f], n, phi);
+    // exactly the resident CTAs (8 x 256 threads per SM), so the grid-stride
+    // loop moves through the grouped pairs as one front and its stores stay in
+    // the few buckets in flight
+    k_phi_scatter<<<grid_for(n, 256, 148 * 8), 256, 0, c.stream>>>(s.k[f][0], s.v[f], n, phi);
     DCX_CHECK_LAUNCH();
     c.launched();
     c.alg(n * 12);

@@ -77,6 +77,7 @@ typedef struct dcx_stats {
     uint64_t tie_groups;      /* phase-4 tie groups (all levels) */
     uint64_t tie_elements;    /* elements in phase-4 tie groups (all levels) */
     uint64_t lookback_gave_up;/* radix-pass CTAs whose bounded look-back wait ran out */
+    uint64_t pool_growth_bytes;/* device memory the allocation pool had to add during the build */
 } dcx_stats;
 
 /* ---- context --------------------------------------------------------------- */
