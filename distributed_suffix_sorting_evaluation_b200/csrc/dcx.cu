@@ -543,25 +543,55 @@ static DBuf<T> upload(Ctx& c, const std::vector<T>& v) {
 // Tie groups: maximal runs of the sorted order whose elements after the first
 // have head 0, binned by size class (tie_class) into gstart/gsize.
 struct TieGroups {
+    bool complete = false;  // the groups hold every tie of the final head flags (tie break may split them)
     uint64_t G = 0;
     std::vector<uint32_t> counts;  // groups per class
     std::vector<uint64_t> off;     // first group of each class in gstart/gsize
     DBuf<uint32_t> gstart, gsize;
 };
 
+static TieGroups bin_groups(Ctx& c, uint64_t G, const uint32_t* starts, const uint32_t* ends);
+
 static TieGroups group_ties(Ctx& c, const uint8_t* head, uint64_t N) {
-    TieGroups tg;
     DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1);
     OpGroups op{head, N, starts.get(), ends.get()};
     const uint64_t tot = device_scan<uint64_t>(c, op, N);
     c.alg(N);
-    tg.G = tot & 0xffffffffull;
+    return bin_groups(c, tot & 0xffffffffull, starts.get(), ends.get());
+}
+
+// Tie groups found inside parent groups that hold every tie (the round-0
+// groups of the window sort): a walk over the parents' head flags instead of a
+// scan of all N flags.
+static TieGroups group_ties_within(Ctx& c, const uint8_t* head, const TieGroups& parents) {
+    const uint64_t Gp = parents.G;
+    uint64_t elems = 0;  // an upper bound on the sub-groups: half the parents' elements
+    for (int k = 0; k < TIE_CLASSES - 1; k++) elems += (uint64_t)parents.counts[k] << (k + 1);
+    const uint64_t cap = elems / 2 + 1;
+    DBuf<uint32_t> starts(&c, cap), ends(&c, cap), cnt(&c, 1);
+    DCX_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, c.stream));
+    if (Gp) {
+        k_subgroups<<<grid_for(Gp, 256, 148 * 16), 256, 0, c.stream>>>(Gp, parents.gstart.get(), parents.gsize.get(),
+                                                                       head, starts.get(), ends.get(), cnt.get());
+        DCX_CHECK_LAUNCH();
+        c.launched();
+        c.alg(elems + Gp * 8);
+    }
+    const uint32_t G = d2h_scalar(c, cnt.get());
+    if (G > cap) throw Error(DCX_ERR_INTERNAL, "more tie groups than the bound");
+    return bin_groups(c, G, starts.get(), ends.get());
+}
+
+// Tie groups (start, end) binned by size class into gstart/gsize.
+static TieGroups bin_groups(Ctx& c, uint64_t G, const uint32_t* starts, const uint32_t* ends) {
+    TieGroups tg;
+    tg.G = G;
     tg.counts.assign(TIE_CLASSES, 0);
     tg.off.assign(TIE_CLASSES + 1, 0);
     if (tg.G == 0) return tg;
     DBuf<uint32_t> cnt(&c, 2 * TIE_CLASSES);
     DCX_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * TIE_CLASSES * 4, c.stream));
-    k_tie_classify<<<grid_for(tg.G, 256), 256, 0, c.stream>>>(tg.G, starts.get(), ends.get(), cnt.get());
+    k_tie_classify<<<grid_for(tg.G, 256), 256, 0, c.stream>>>(tg.G, starts, ends, cnt.get());
     DCX_CHECK_LAUNCH();
     DCX_CUDA(cudaMemcpyAsync(tg.counts.data(), cnt.get(), TIE_CLASSES * 4, cudaMemcpyDeviceToHost, c.stream));
     DCX_CUDA(cudaStreamSynchronize(c.stream));
@@ -573,10 +603,10 @@ static TieGroups group_ties(Ctx& c, const uint8_t* head, uint64_t N) {
     DCX_CUDA(cudaMemcpyAsync(cnt.get() + TIE_CLASSES, cursor.data(), TIE_CLASSES * 4, cudaMemcpyHostToDevice, c.stream));
     tg.gstart = DBuf<uint32_t>(&c, tg.G);
     tg.gsize = DBuf<uint32_t>(&c, tg.G);
-    k_tie_bin<<<grid_for(tg.G, 256), 256, 0, c.stream>>>(tg.G, starts.get(), ends.get(), cnt.get() + TIE_CLASSES,
+    k_tie_bin<<<grid_for(tg.G, 256), 256, 0, c.stream>>>(tg.G, starts, ends, cnt.get() + TIE_CLASSES,
                                                           tg.gstart.get(), tg.gsize.get());
     DCX_CHECK_LAUNCH();
-    c.launched(4);
+    c.launched(2);
     return tg;
 }
 
@@ -659,7 +689,8 @@ static void refine_seg_class(Ctx& c, const CharT* text, SegView sv, const uint32
 // ---------------------------------------------------------------------------
 template <typename CharT>
 static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64_t* d_start, uint64_t B, uint32_t L,
-                         int depth, DBuf<uint32_t>& sa, DBuf<uint8_t>& head, DBuf<uint32_t>& segw) {
+                         int depth, DBuf<uint32_t>& sa, DBuf<uint8_t>& head, DBuf<uint32_t>& segw,
+                         TieGroups* parents) {
     const uint64_t N = sg.N();
     const uint32_t K = sg.K();
     const bool SEGK = K > 1;
@@ -885,6 +916,19 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         DCX_CHECK_LAUNCH();
         c.launched();
     }
+    // The round-0 groups hold every tie that is left: the tie break looks for its
+    // groups inside them instead of scanning all N head flags again.
+    if (parents) {
+        if (!round0_ties) {
+            parents->complete = true;
+            parents->G = 0;
+            parents->counts.assign(TIE_CLASSES, 0);
+            parents->off.assign(TIE_CLASSES + 1, 0);
+        } else if (!tg.counts.empty() && tg.counts[TIE_CLASSES - 1] == 0) {
+            *parents = std::move(tg);
+            parents->complete = true;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -977,8 +1021,8 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
 }
 
 static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, const uint32_t* rank_text,
-                      const DcHost& dc, TieSeg ts) {
-    TieGroups tg = group_ties(c, head, N);
+                      const DcHost& dc, TieSeg ts, const TieGroups* parents) {
+    TieGroups tg = parents ? group_ties_within(c, head, *parents) : group_ties(c, head, N);
     const uint64_t G = tg.G;
     if (G == 0) return;
     const std::vector<uint32_t>& counts = tg.counts;
@@ -1104,7 +1148,8 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
     // ---- phase 1: window sort
     DBuf<uint32_t> sa, segw;
     DBuf<uint8_t> head;
-    sort_windows<CharT>(c, text, sg, d_start.get(), B, L, depth, sa, head, segw);
+    TieGroups parents;  // round-0 tie groups, kept for the tie break
+    sort_windows<CharT>(c, text, sg, d_start.get(), B, L, depth, sa, head, segw, &parents);
     const uint32_t* segw_p = K > 1 ? segw.get() : nullptr;
 
     // ---- phase 2: names
@@ -1335,11 +1380,26 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
     cudaEventRecord(ev[2], c.stream);
 
     // ---- phase 4: tie groups, then emit
-    tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc, TieSeg{segw_p, d_start.get(), d_rbase.get()});
+    tie_break(c, sa.get(), head.get(), N, rank_text.get(), dc, TieSeg{segw_p, d_start.get(), d_rbase.get()},
+              parents.complete ? &parents : nullptr);
+    parents = TieGroups{};
     head.reset();
     rank_text.reset();
     if (K == 1 && sg.out_base.empty()) {
-        k_emit<<<grid_for(N / 4 + 1, 256), 256, 0, c.stream>>>(sa.get(), N - 1, sa_out, out_width);
+        const uint64_t n_out = N - 1;
+        if (out_width == 40 && ((uintptr_t)sa_out & 15) == 0 && n_out >= EMIT40_TILE) {
+            // full 1024-entry tiles through shared memory, the rest entry by entry
+            const uint64_t head_n = n_out / EMIT40_TILE * EMIT40_TILE;
+            k_emit40<<<grid_for(head_n / EMIT40_TILE, 1, 148 * 8), 256, 0, c.stream>>>(sa.get(), n_out,
+                                                                                      (uint8_t*)sa_out);
+            DCX_CHECK_LAUNCH();
+            c.launched();
+            if (head_n < n_out)
+                k_emit<<<1, 256, 0, c.stream>>>(sa.get() + head_n, n_out - head_n,
+                                                (uint8_t*)sa_out + 5 * head_n, out_width);
+        } else {
+            k_emit<<<grid_for(N / 4 + 1, 256), 256, 0, c.stream>>>(sa.get(), N - 1, sa_out, out_width);
+        }
     } else {
         k_emit_seg<<<grid_for(N, 256), 256, 0, c.stream>>>(sa.get(), segw_p, N, ls, sa_out, out_width);
     }

@@ -616,6 +616,60 @@ __global__ void k_tie_classify(uint64_t G, const uint32_t* __restrict__ starts, 
     if (threadIdx.x < TIE_CLASSES && c[threadIdx.x]) atomicAdd(&counts[threadIdx.x], c[threadIdx.x]);
 }
 
+// Tie groups (runs of two or more equal windows) inside parent groups that
+// hold every tie: one thread per parent group walks its head flags twice
+// (count, then emit); the runs are appended as (start, end) in any order, one
+// atomic reservation per warp.  Every lane runs the same number of rounds.
+__global__ void k_subgroups(uint64_t Gp, const uint32_t* __restrict__ pstart, const uint32_t* __restrict__ psize,
+                            const uint8_t* __restrict__ head, uint32_t* __restrict__ out_start,
+                            uint32_t* __restrict__ out_end, uint32_t* __restrict__ count) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t first = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t rounds = (Gp + stride - 1) / stride;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t r = 0; r < rounds; r++) {
+        const uint64_t g = first + r * stride;
+        uint32_t st = 0, sz = 0, nsub = 0;
+        if (g < Gp) {
+            st = pstart[g];
+            sz = psize[g];
+            uint32_t run = 1;
+            for (uint32_t k = 1; k < sz; k++) {
+                if (head[st + k]) {
+                    nsub += run > 1;
+                    run = 1;
+                } else {
+                    run++;
+                }
+            }
+            nsub += run > 1;
+        }
+        uint32_t incl = nsub;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t base = 0;
+        if (lane == 31 && total) base = atomicAdd(count, total);
+        base = __shfl_sync(0xffffffffu, base, 31) + incl - nsub;
+        if (nsub) {
+            uint32_t a = st;
+            for (uint32_t k = 1; k <= sz; k++) {
+                if (k == sz || head[st + k]) {
+                    if (st + k - 1 > a) {
+                        out_start[base] = a;
+                        out_end[base] = st + k - 1;
+                        base++;
+                    }
+                    a = st + k;
+                }
+            }
+        }
+    }
+}
+
 // Bins tie groups by size class.  Cursor updates are aggregated per warp: the
 // lanes holding the same class elect one lane that reserves their slots.
 __global__ void k_tie_bin(uint64_t G, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
@@ -703,6 +757,33 @@ __global__ void k_emit(const uint32_t* __restrict__ sa_full, uint64_t n, void* _
     }
 }
 
+
+// 40-bit output through shared memory: each thread packs four entries into
+// five words (conflict-free: thread t writes words 5t..5t+4), then the CTA
+// writes its 1024 entries (5120 bytes) with coalesced 16-byte stores.  The
+// output must be 16-byte aligned; entries past the last full tile are written
+// by k_emit's byte path (`tail_from` = first entry not written here).
+constexpr uint32_t EMIT40_TILE = 1024;
+__global__ __launch_bounds__(256) void k_emit40(const uint32_t* __restrict__ sa_full, uint64_t n,
+                                                uint8_t* __restrict__ out) {
+    __shared__ __align__(16) uint32_t sw[EMIT40_TILE * 5 / 4];
+    const uint64_t tiles = n / EMIT40_TILE;
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t k0 = t * EMIT40_TILE + 4 * threadIdx.x;
+        const uint32_t e0 = sa_full[k0 + 1], e1 = sa_full[k0 + 2], e2 = sa_full[k0 + 3], e3 = sa_full[k0 + 4];
+        uint32_t* o = sw + 5 * threadIdx.x;
+        o[0] = e0;
+        o[1] = e1 << 8;
+        o[2] = (e1 >> 24) | (e2 << 16);
+        o[3] = (e2 >> 16) | (e3 << 24);
+        o[4] = e3 >> 8;
+        __syncthreads();
+        uint4* dst = reinterpret_cast<uint4*>(out + t * EMIT40_TILE * 5);
+        const uint4* src = reinterpret_cast<const uint4*>(sw);
+        for (uint32_t q = threadIdx.x; q < EMIT40_TILE * 5 / 16; q += blockDim.x) dst[q] = src[q];
+        __syncthreads();
+    }
+}
 
 // Several texts: sorted element k belongs to text s = segw[k]; text s's elements
 // occupy sorted slots [start[s], start[s+1]) with its empty suffix first, so
