@@ -324,11 +324,9 @@ def run_split(args, world, rank, local):
     if not dist.is_initialized():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev,
                                 world_size=world, rank=rank)
-    w = dict(W.WORKLOADS[args.workload])
-    if args.text_mib:
-        w["n"] = args.text_mib << 20
+    w, gen_kw, label = _single_workload(args)
     n = int(w["n"])
-    text = getattr(W, w["gen"])(n, seed=w["seed"])  # the same text on every rank
+    text = getattr(W, w["gen"])(n, seed=w["seed"], **gen_kw)  # the same text on every rank
     lo, hi = rank * n // world, (rank + 1) * n // world
     h_block = torch.from_numpy(text[lo:hi].copy()).pin_memory()
     d_block = h_block.to(dev)
@@ -384,7 +382,7 @@ def run_split(args, world, rank, local):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
             "data": W.DESCRIPTIONS[args.workload],
-            "config": {"workload": args.workload if not args.text_mib else f"{args.workload}@{args.text_mib}MiB",
+            "config": {"workload": label,
                        "text_bytes": n, "dc": w["dc"], "sa_width": 64,
                        "l2_flush": "inputs larger than L2", "parallelism": f"split text over {world} ranks"},
             "e2e": {"value": round(n / GiB / (ms_e2e / 1000.0), 4), "unit": "GiB/s",
@@ -407,14 +405,12 @@ def run_gpu(args, world, rank, local):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    w = dict(W.WORKLOADS[args.workload])
-    if args.text_mib:
-        w["n"] = args.text_mib << 20
+    w, gen_kw, label = _single_workload(args)
     n = int(w["n"])
     dc, width = w["dc"], w["sa_width"]
     wb = width // 8
     host_text = torch.empty(n, dtype=torch.uint8, pin_memory=True)
-    getattr(W, w["gen"])(n, seed=w["seed"] + 1000 * rank, out=host_text.numpy())
+    getattr(W, w["gen"])(n, seed=w["seed"] + 1000 * rank, out=host_text.numpy(), **gen_kw)
     d_text = host_text.to(f"cuda:{local}")
     d_sa = torch.empty(n * wb, dtype=torch.uint8, device=f"cuda:{local}")
     host_sa = torch.empty(n * wb, dtype=torch.uint8, pin_memory=True)
@@ -556,7 +552,7 @@ def run_gpu(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": W.DESCRIPTIONS[args.workload],
-            "config": {"workload": args.workload if not args.text_mib else f"{args.workload}@{args.text_mib}MiB",
+            "config": {"workload": label,
                        "text_bytes": n, "dc": dc, "packing": True, "sa_width": width,
                        "l2_flush": "inputs larger than L2 (1 GiB text)",
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
@@ -1015,6 +1011,21 @@ def run_serve(args, world, rank, local):
     return 0
 
 
+def _single_workload(args):
+    """The single-text workload's parameters, generator arguments and name,
+    with the size overrides of profiling captures applied."""
+    w = dict(W.WORKLOADS[args.workload])
+    label = args.workload
+    if args.text_mib:
+        w["n"] = args.text_mib << 20
+        label += f"@{args.text_mib}MiB"
+    gen_kw = {}
+    if args.base_kib and w["gen"] == "pangenome":
+        gen_kw["base_len"] = args.base_kib << 10
+        label += f",base{args.base_kib}KiB"
+    return w, gen_kw, label
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1023,6 +1034,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--text-mib", type=int, default=0, help="override the text size (profiling captures)")
+    ap.add_argument("--base-kib", type=int, default=0,
+                    help="pangenome base length (a smaller text with the full-size copy count, for profiling captures)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample-mib", type=int, default=0,
                     help="text prefix the CPU baseline builds (0 = the whole text)")
