@@ -1014,6 +1014,7 @@ def run_serve(args, world, rank, local):
 def _single_workload(args):
     """The single-text workload's parameters, generator arguments and name,
     with the size overrides of profiling captures applied."""
+    from distributed_suffix_sorting_evaluation_b200 import workloads as W
     w = dict(W.WORKLOADS[args.workload])
     label = args.workload
     if args.text_mib:

@@ -405,16 +405,27 @@ static const DcHost& get_dc(Ctx& c, uint32_t X) {
 // ---------------------------------------------------------------------------
 // Radix sort driver.  Keys/values in buffer 0, digit histograms of all 4*kw
 // passes in c.d_hist.  Passes whose digit is constant are skipped.  Returns the
-// index (0/1) of the buffer holding the sorted data.
+// index (0/1) of the buffer holding the sorted data.  With digit_shift >= 0 it
+// runs the single pass on the 8-bit digit (key word 0 >> digit_shift) & 255,
+// whose histogram is the first RADIX words of c.d_hist (digit_shift <= 24).
 // ---------------------------------------------------------------------------
+// Shift of the 8-bit digit that cuts [0, span) into 256 contiguous ranges (the
+// two-step scatters group their stores by it).
+static uint32_t top_digit_shift(uint64_t span) {
+    uint32_t bits = 0;
+    while (bits < 32 && ((span - 1) >> bits)) bits++;
+    return bits > 8 ? bits - 8 : 0;
+}
+
 struct SortSpace {
     uint32_t* k[2][MAX_KEY_WORDS] = {};
     uint32_t* v[2] = {};
 };
 
-static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
+static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s, int digit_shift = -1) {
     if (kw > 3) throw Error(DCX_ERR_INTERNAL, "radix keys wider than 3 words");
-    const uint32_t passes = 4 * kw;
+    if (digit_shift > 24) throw Error(DCX_ERR_INTERNAL, "single-pass digit outside key word 0");
+    const uint32_t passes = digit_shift >= 0 ? 1 : 4 * kw;
     // histograms in and digit bases out through pinned staging (PINNED_WORDS words each)
     uint32_t* h = reinterpret_cast<uint32_t*>(c.h_pinned);
     uint32_t* hb = h + PINNED_WORDS / 2;
@@ -430,7 +441,7 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         // one digit value for all keys, or a digit the producer left uncounted
         // because it is zero in every key
         if ((uint64_t)mx == count || sum == 0) continue;
-        run.push_back(p);
+        run.push_back(digit_shift >= 0 ? (uint32_t)digit_shift : p * RADIX_BITS);
         uint32_t acc = 0;
         for (int d = 0; d < RADIX; d++) {
             bases.push_back(acc);
@@ -486,7 +497,7 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s) {
         a.vals_out = s.v[cur ^ 1];
         a.kw = kw;
         a.n = count;
-        a.shift = run[i] * RADIX_BITS;
+        a.shift = run[i];
         a.digit_base = c.d_base + i * RADIX;
         a.lookback = c.d_lookback;
         a.tile_counter = c.d_tiles + i;
@@ -1180,10 +1191,8 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
         c.launched();
         c.alg(m * 21);
     } else {
-        // group the records by the second-highest byte of their slot first
-        uint32_t bits = 0;
-        while (bits < 32 && ((slots - 1) >> bits)) bits++;
-        const uint32_t byte = (bits + 7) / 8 >= 2 ? (bits + 7) / 8 - 2 : 0;
+        // group the records by the top 8 bits of their slot first
+        const uint32_t shift = top_digit_shift(slots);
         SortSpace s;
         DBuf<uint32_t> rk[2][2], rv[2];
         for (int b = 0; b < 2; b++) {
@@ -1197,11 +1206,11 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
         DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
         k_sample_records<<<grid_for(m, 256, 148 * 8), 256, 0, c.stream>>>(m, s_pos.get(), s_seg.get(), name.get(),
                                                                           uniq.get(), dfl.get(), ls, s.k[0][0],
-                                                                          s.k[0][1], s.v[0], c.d_hist, byte);
+                                                                          s.k[0][1], s.v[0], c.d_hist, shift);
         DCX_CHECK_LAUNCH();
         c.launched();
         c.alg(m * 21);
-        const int f = radix_sort(c, 2, m, s);
+        const int f = radix_sort(c, 2, m, s, (int)shift);
         // resident CTAs only: one front through the grouped records (see build_phi)
         k_scatter_records<<<grid_for(m, 256, 148 * 8), 256, 0, c.stream>>>(m, s.k[f][0], s.k[f][1], s.v[f],
                                                                            srec.get());
@@ -1317,12 +1326,37 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
             DBuf<uint32_t> d_rt = upload(c, rec_text);
             DBuf<uint32_t> rank_of;
             if (any_discard) rank_of = DBuf<uint32_t>(&c, total2);
-            k_after_recursion<<<grid_for(total2, 256), 256, 0, c.stream>>>(total2, sa2.get(), d_o2.get(), R,
-                                                                           d_rt.get(), dfl.get(), ls, rank_text.get(),
-                                                                           any_discard ? rank_of.get() : nullptr);
-            DCX_CHECK_LAUNCH();
-            c.launched();
-            c.alg(total2 * 12);
+            if (total2 <= (1u << 20)) {  // 4 MB of ranks: a direct scatter stays in L2
+                k_after_recursion<<<grid_for(total2, 256), 256, 0, c.stream>>>(total2, sa2.get(), d_o2.get(), R,
+                                                                               d_rt.get(), dfl.get(), ls,
+                                                                               rank_text.get(),
+                                                                               any_discard ? rank_of.get() : nullptr);
+                DCX_CHECK_LAUNCH();
+                c.launched();
+                c.alg(total2 * 12);
+            } else {
+                // group the rank stores by the top 8 bits of their destination first
+                const uint32_t shift = top_digit_shift(std::max<uint64_t>(slots, any_discard ? total2 : 0));
+                SortSpace s;
+                DBuf<uint32_t> rk1(&c, total2), rv0(&c, total2), rv1(&c, total2);
+                s.k[0][0] = sa2.get();  // the records overwrite sa2 in place, element by element
+                s.k[1][0] = rk1.get();
+                s.v[0] = rv0.get();
+                s.v[1] = rv1.get();
+                DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
+                k_after_records<<<grid_for(total2, 256, 148 * 8), 256, 0, c.stream>>>(
+                    total2, sa2.get(), d_o2.get(), R, d_rt.get(), dfl.get(), ls, s.k[0][0], s.v[0], c.d_hist, shift);
+                DCX_CHECK_LAUNCH();
+                c.launched();
+                c.alg(total2 * 12);
+                const int f = radix_sort(c, 1, total2, s, (int)shift);
+                // resident CTAs only: one front through the grouped records
+                k_scatter_ranks<<<grid_for(total2, 256, 148 * 8), 256, 0, c.stream>>>(
+                    total2, s.k[f][0], s.v[f], rank_text.get(), any_discard ? rank_of.get() : nullptr);
+                DCX_CHECK_LAUNCH();
+                c.launched();
+                c.alg(total2 * 12);
+            }
             sa2.reset();
             if (any_discard) {
                 // non-unique samples of discarding texts: sort by (name, rank2) (pdcx.hpp:296-346)
@@ -2005,8 +2039,8 @@ static bool check_sa_file(Ctx& c, const uint8_t* text, uint64_t n, const char* p
 }
 
 // phi[SA[k]] = SA[k-1]: a direct scatter while phi fits L2 (16 MB), else the
-// two-step form (records, one radix pass on the second-highest byte of SA[k],
-// an L2-local scatter).
+// two-step form (records, one radix pass on the top 8 bits of SA[k], an
+// L2-local scatter).
 static void build_phi(Ctx& c, const uint32_t* sa32, uint64_t n, uint32_t* phi) {
     if (n <= (1u << 22)) {
         k_phi<<<grid_for(n, 256), 256, 0, c.stream>>>(sa32, n, phi);
@@ -2015,9 +2049,7 @@ static void build_phi(Ctx& c, const uint32_t* sa32, uint64_t n, uint32_t* phi) {
         c.alg(n * 12);
         return;
     }
-    uint32_t bits = 0;
-    while (bits < 32 && ((n - 1) >> bits)) bits++;
-    const uint32_t byte = (bits + 7) / 8 >= 2 ? (bits + 7) / 8 - 2 : 0;
+    const uint32_t shift = top_digit_shift(n);
     SortSpace s;
     DBuf<uint32_t> pk[2], pv[2];
     for (int b = 0; b < 2; b++) {
@@ -2027,11 +2059,11 @@ static void build_phi(Ctx& c, const uint32_t* sa32, uint64_t n, uint32_t* phi) {
         s.v[b] = pv[b].get();
     }
     DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
-    k_phi_records<<<grid_for(n, 256, 148 * 8), 256, 0, c.stream>>>(sa32, n, s.k[0][0], s.v[0], c.d_hist, byte);
+    k_phi_records<<<grid_for(n, 256, 148 * 8), 256, 0, c.stream>>>(sa32, n, s.k[0][0], s.v[0], c.d_hist, shift);
     DCX_CHECK_LAUNCH();
     c.launched();
     c.alg(n * 16);
-    const int f = radix_sort(c, 1, n, s);
+    const int f = radix_sort(c, 1, n, s, (int)shift);
     // exactly the resident CTAs (8 x 256 threads per SM), so the grid-stride
     // loop moves through the grouped pairs as one front and its stores stay in
     // the few buckets in flight

@@ -7,13 +7,14 @@
 
 namespace dcx {
 
-// k_phi_records lays out (SA[k], SA[k-1]) and histograms one byte of SA[k];
-// one radix pass on that byte groups the pairs by 1/256 of the position range;
+// k_phi_records lays out (SA[k], SA[k-1]) and histograms the digit
+// (SA[k] >> shift) & 255, the top 8 bits of the position; one radix pass on that
+// digit groups the pairs into 256 contiguous position ranges;
 // k_phi_scatter then stores them in that order, so the stores of concurrent
 // CTAs land in a few megabytes of phi that L2 fills completely before writing
 // back.
 __global__ void k_phi_records(const uint32_t* __restrict__ sa32, uint64_t n, uint32_t* __restrict__ dst,
-                              uint32_t* __restrict__ val, uint32_t* __restrict__ hist, uint32_t byte) {
+                              uint32_t* __restrict__ val, uint32_t* __restrict__ hist, uint32_t shift) {
     __shared__ uint32_t h[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
     __syncthreads();
@@ -21,11 +22,11 @@ __global__ void k_phi_records(const uint32_t* __restrict__ sa32, uint64_t n, uin
         const uint32_t d = sa32[k];
         dst[k] = d;
         val[k] = k ? sa32[k - 1] : PHI_NONE;
-        atomicAdd(&h[(d >> (8 * byte)) & 255u], 1u);
+        atomicAdd(&h[(d >> shift) & 255u], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 256; i += blockDim.x)
-        if (h[i]) atomicAdd(&hist[byte * 256 + i], h[i]);
+        if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
 __global__ void k_phi_scatter(const uint32_t* __restrict__ dst, const uint32_t* __restrict__ val, uint64_t n,

@@ -367,15 +367,16 @@ __global__ void k_scatter_samples(uint64_t m, const uint32_t* __restrict__ s_pos
 
 // The same records in two steps for large levels, so that no store is a lone
 // 8-byte write into a 32-byte sector: k_sample_records lays each sample out as
-// (slot, name, unique | j << 1) and histograms one byte of the slot; one radix
-// pass on that byte groups the samples by 1/256 of the slot range; then
+// (slot, name, unique | j << 1) and histograms the top 8 bits of the slot
+// ((slot >> shift) & 255); one radix pass on that digit groups the samples into
+// 256 contiguous slot ranges; then
 // k_scatter_records stores them in that order, so the stores of concurrent
 // CTAs land in a few megabytes that L2 fills completely before writing back.
 __global__ void k_sample_records(uint64_t m, const uint32_t* __restrict__ s_pos, const uint32_t* __restrict__ s_seg,
                                  const uint32_t* __restrict__ name, const uint8_t* __restrict__ uniq,
                                  const DcFlags* __restrict__ f, LevelSeg ls, uint32_t* __restrict__ slot_out,
                                  uint32_t* __restrict__ name_out, uint32_t* __restrict__ hi_out,
-                                 uint32_t* __restrict__ hist, uint32_t byte) {
+                                 uint32_t* __restrict__ hist, uint32_t shift) {
     __shared__ uint32_t h[RADIX];
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
     __syncthreads();
@@ -385,11 +386,11 @@ __global__ void k_sample_records(uint64_t m, const uint32_t* __restrict__ s_pos,
         slot_out[j] = k;
         name_out[j] = name[j];
         hi_out[j] = (uint32_t)uniq[j] | ((uint32_t)j << 1);
-        atomicAdd(&h[(k >> (8 * byte)) & (RADIX - 1)], 1u);
+        atomicAdd(&h[(k >> shift) & (RADIX - 1)], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x)
-        if (h[i]) atomicAdd(&hist[byte * RADIX + i], h[i]);
+        if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
 __global__ void k_scatter_records(uint64_t m, const uint32_t* __restrict__ slot, const uint32_t* __restrict__ lo,
@@ -501,6 +502,55 @@ __global__ void k_after_recursion(uint64_t total2, const uint32_t* __restrict__ 
         } else {
             rank_of[ls.kbase[s] + ql] = (uint32_t)(k + 1);
         }
+    }
+}
+
+// Two-step form of k_after_recursion for large levels (the same idea as
+// k_sample_records): every rank store becomes a record (destination, rank |
+// target << 31), target 1 = rank_of, and the top 8 bits of the destination are
+// histogrammed; one radix pass on that digit groups the records into 256
+// contiguous destination ranges, and k_scatter_ranks stores them in that order.  Ranks are
+// below 2^31 (a level has fewer than 2^31 samples), so bit 31 is free.
+// dst_out may be sa2 itself (each element is read, then overwritten, by one thread).
+__global__ void k_after_records(uint64_t total2, const uint32_t* sa2, const uint64_t* __restrict__ o2,
+                                uint32_t R, const uint32_t* __restrict__ rec_text, const DcFlags* __restrict__ f,
+                                LevelSeg ls, uint32_t* dst_out, uint32_t* __restrict__ val_out,
+                                uint32_t* __restrict__ hist, uint32_t shift) {
+    __shared__ uint32_t h[RADIX];
+    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const uint32_t D = f->D;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total2;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = R > 1 ? bsearch_le(o2, R, x) : 0u;
+        const uint32_t s = rec_text[r];
+        const uint64_t k = x - o2[r];
+        const uint64_t ql = sa2[x];
+        uint32_t dst, v = (uint32_t)(k + 1);
+        if (ls.mode[s] == REC_DIRECT) {
+            const uint64_t* sb = ls.sb + (uint64_t)s * (D + 1);
+            uint32_t c = 0;
+            while (c + 1 < D && ql >= sb[c + 1]) c++;
+            dst = (uint32_t)(ls.rbase[s] + (ql - sb[c]) * D + c);
+        } else {
+            dst = (uint32_t)(ls.kbase[s] + ql);
+            v |= 0x80000000u;
+        }
+        dst_out[x] = dst;
+        val_out[x] = v;
+        atomicAdd(&h[(dst >> shift) & (RADIX - 1)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < RADIX; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+__global__ void k_scatter_ranks(uint64_t n, const uint32_t* __restrict__ dst, const uint32_t* __restrict__ val,
+                                uint32_t* __restrict__ rank_text, uint32_t* __restrict__ rank_of) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = val[j];
+        if (v >> 31) rank_of[dst[j]] = v & 0x7fffffffu;
+        else rank_text[dst[j]] = v;
     }
 }
 
