@@ -24,7 +24,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"
 HOST_CXX = "/usr/bin/g++"
 
 SOURCES = ["dcx.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "radix.cuh", "keys.cuh", "segsort.cuh", "small_sa.cuh", "level_kernels.cuh", "lcp.cuh",
+HEADERS = ["common.cuh", "radix.cuh", "keys.cuh", "segsort.cuh", "warpsort.cuh", "small_sa.cuh", "level_kernels.cuh", "lcp.cuh",
            "lcp_scatter.cuh", "bwt.cuh", "gsa.cuh", "serve.cuh"]
 
 

@@ -36,6 +36,7 @@
 #include "radix.cuh"
 #include "segsort.cuh"
 #include "small_sa.cuh"
+#include "warpsort.cuh"
 #include "lcp.cuh"
 #include "lcp_scatter.cuh"
 #include "bwt.cuh"
@@ -676,6 +677,23 @@ static void refine_small_w(Ctx& c, const CharT* text, SegView sv, const uint32_t
     sub(4, std::integral_constant<int, 32>{});
 }
 
+// Groups of one size class (33-64, 65-128 or 129-256 elements: E = 2, 4, 8)
+// refined by one window word, one warp per group.
+template <int E, typename CharT>
+static void refine_warp_class(Ctx& c, const CharT* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
+                              int cls, uint32_t* sa, uint8_t* head, const RefineSegPlan& plan) {
+    const uint64_t ng = tg.counts[cls];
+    if (!ng) return;
+    auto kern = k_refine_warpsort<E, CharT>;
+    int per_sm = 0;
+    DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * WSORT_WARPS, 0));
+    const uint64_t grid = std::min<uint64_t>(div_up(ng, WSORT_WARPS), 148ull * std::max(per_sm, 1));
+    kern<<<(unsigned)grid, 32 * WSORT_WARPS, 0, c.stream>>>(text, sv, segw, tg.gstart.get() + tg.off[cls],
+                                                            tg.gsize.get() + tg.off[cls], ng, sa, head, plan);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+}
+
 template <int C, int T, typename CharT>
 static void refine_seg_class(Ctx& c, const CharT* text, SegView sv, const uint32_t* segw, const TieGroups& tg,
                              int cls_lo, int cls_hi, uint32_t* sa, uint8_t* head, const RefineSegPlan& plan) {
@@ -838,8 +856,14 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
                 case 5: refine_small_w<5>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
                 default: refine_small_w<6>(c, t8, sv, sw, tg, sa.get(), hd, plan); break;
             }
-            refine_seg_class<64, 32>(c, t8, sv, sw, tg, 5, 5, sa.get(), hd, plan);
-            refine_seg_class<256, 128>(c, t8, sv, sw, tg, 6, 7, sa.get(), hd, plan);
+            if (W == 1) {  // one window word: one warp per group, elements in registers
+                refine_warp_class<2>(c, t8, sv, sw, tg, 5, sa.get(), hd, plan);
+                refine_warp_class<4>(c, t8, sv, sw, tg, 6, sa.get(), hd, plan);
+                refine_warp_class<8>(c, t8, sv, sw, tg, 7, sa.get(), hd, plan);
+            } else {
+                refine_seg_class<64, 32>(c, t8, sv, sw, tg, 5, 5, sa.get(), hd, plan);
+                refine_seg_class<256, 128>(c, t8, sv, sw, tg, 6, 7, sa.get(), hd, plan);
+            }
             refine_seg_class<1024, 512>(c, t8, sv, sw, tg, 8, 9, sa.get(), hd, plan);
             refine_seg_class<2048, 512>(c, t8, sv, sw, tg, 10, 10, sa.get(), hd, plan);
             const uint64_t small = tg.off[TIE_CLASSES - 1];  // groups of at most 2048
@@ -957,13 +981,13 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         if (!g) return;
         const uint64_t warps = div_up(g, 32 / Wv);
         const uint64_t blocks = div_up(warps * 32, 256);
-        k_tie_warp<D, Wv><<<(unsigned)blocks, 256, 0, c.stream>>>(gstart + off[cls], gsize + off[cls], (uint32_t)g,
+        k_tie_warp<D, Wv><<<(unsigned)blocks, 256, tie_tab_smem(X), c.stream>>>(gstart + off[cls], gsize + off[cls], (uint32_t)g,
                                                                   sa, rank_text, dcd, ts);
         DCX_CHECK_LAUNCH();
         c.launched();
     };
     if (counts[0]) {  // pairs
-        k_tie_pair<<<grid_for(counts[0], 256, 148 * 16), 256, 0, c.stream>>>(gstart + off[0], counts[0], sa, rank_text,
+        k_tie_pair<<<grid_for(counts[0], 256, 148 * 16), 256, tie_tab_smem(X), c.stream>>>(gstart + off[0], counts[0], sa, rank_text,
                                                                            dcd, ts);
         DCX_CHECK_LAUNCH();
         c.launched();
@@ -985,9 +1009,24 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
         DCX_CHECK_LAUNCH();
         c.launched();
     };
-    cta_launch(gstart + off[5], gsize + off[5], counts[5], std::integral_constant<int, 64>{});
-    cta_launch(gstart + off[6], gsize + off[6], counts[6], std::integral_constant<int, 128>{});
-    cta_launch(gstart + off[7], gsize + off[7], counts[7], std::integral_constant<int, 256>{});
+    // 33-64, 65-128, 129-256 elements: one warp per group
+    auto warpsort_launch = [&](int cls, auto Ec) {
+        constexpr int E = decltype(Ec)::value;
+        const uint64_t g = counts[cls];
+        if (!g) return;
+        const size_t shm = tie_warpsort_smem<D, E>(X);
+        DCX_CUDA(cudaFuncSetAttribute(k_tie_warpsort<D, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        int per_sm = 0;
+        DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tie_warpsort<D, E>, 32 * WSORT_WARPS, shm));
+        const uint64_t grid = std::min<uint64_t>(div_up(g, WSORT_WARPS), 148ull * std::max(per_sm, 1));
+        k_tie_warpsort<D, E><<<(unsigned)grid, 32 * WSORT_WARPS, shm, c.stream>>>(gstart + off[cls], gsize + off[cls], g,
+                                                                                sa, rank_text, dcd, ts);
+        DCX_CHECK_LAUNCH();
+        c.launched();
+    };
+    warpsort_launch(5, std::integral_constant<int, 2>{});
+    warpsort_launch(6, std::integral_constant<int, 4>{});
+    warpsort_launch(7, std::integral_constant<int, 8>{});
     cta_launch(gstart + off[8], gsize + off[8], counts[8], std::integral_constant<int, 512>{});
     cta_launch(gstart + off[9], gsize + off[9], counts[9], std::integral_constant<int, 1024>{});
     cta_launch(gstart + off[10], gsize + off[10], counts[10], std::integral_constant<int, 2048>{});

@@ -394,13 +394,25 @@ __global__ __launch_bounds__(THREADS) void k_refine_seg(const CharT* __restrict_
     for (uint64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const uint32_t start = gstart[g], size = gsize[g];
         const uint64_t end = seg_end(sv, segw ? segw[start] : 0u);
-        for (uint32_t i = threadIdx.x; i < (uint32_t)C; i += THREADS) {
-            s_idx[i] = (uint16_t)i;
-            if (i < size) {
-                const uint32_t p = sa[start + i];
-                s_pos[i] = p;
+        // all positions first, then all windows: the loads of a thread's
+        // elements are independent and overlap
+        constexpr int PER = C / THREADS;
+        static_assert(PER * THREADS == C, "C is a multiple of THREADS");
+        uint32_t pj[PER];
 #pragma unroll
-                for (int w = 0; w < W; w++) s_key[w][i] = window_value_t(text, (uint64_t)p + plan.off[w], end, plan.rp[w]);
+        for (int j = 0; j < PER; j++) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            s_idx[i] = (uint16_t)i;
+            pj[j] = i < size ? sa[start + i] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            if (i < size) {
+                s_pos[i] = pj[j];
+#pragma unroll
+                for (int w = 0; w < W; w++)
+                    s_key[w][i] = window_value_t(text, (uint64_t)pj[j] + plan.off[w], end, plan.rp[w]);
             }
         }
         __syncthreads();

@@ -9,8 +9,9 @@
 // for the whole window (L >= X > d), so only the rank comparison remains.
 //
 // Groups are binned by size: up to 32 elements are sorted by a bitonic network
-// inside W = 2..32 lanes of a warp (several groups per warp); up to 2048 by a
-// bitonic network in shared memory of one CTA; larger groups are cut into
+// inside W = 2..32 lanes of a warp (several groups per warp); 33..256 by one
+// warp each (k_tie_warpsort, warpsort.cuh); up to 2048 by a bitonic network in
+// shared memory of one CTA; larger groups are cut into
 // 2048-chunks sorted the same way and then merged in rounds where every element
 // finds its output slot by binary search in the partner run.
 #pragma once
@@ -49,21 +50,24 @@ __device__ __forceinline__ void tie_bases(const TieSeg& ts, uint64_t sorted_slot
 template <int D>
 struct Rec {
     uint32_t pos;  // text-local position
+    uint32_t res;  // pos mod X
     uint32_t r[D];
 };
 
 template <int D>
-__device__ __forceinline__ Rec<D> load_rec(uint32_t pos, const uint32_t* __restrict__ rank_text, uint32_t X,
+__device__ __forceinline__ Rec<D> load_rec(uint32_t pos, const uint32_t* __restrict__ rank_text, const FastDiv& fx,
                                            const uint32_t* next_rank) {
     Rec<D> r;
     r.pos = pos;
+    r.res = 0;
     if (pos == INVALID_POS) {
 #pragma unroll
         for (int k = 0; k < D; k++) r.r[k] = 0;
         return r;
     }
-    const uint32_t q = pos / X;
-    const uint64_t rp = (uint64_t)q * D + next_rank[pos - q * X];
+    uint32_t q;
+    fdivmod(pos, fx, q, r.res);
+    const uint64_t rp = (uint64_t)q * D + next_rank[r.res];
 #pragma unroll
     for (int k = 0; k < D; k++) r.r[k] = __ldg(rank_text + rp + k);
     return r;
@@ -83,7 +87,7 @@ template <int D>
 __device__ __forceinline__ bool dc_less(const Rec<D>& a, const Rec<D>& b, uint32_t X, const uint16_t* tab) {
     if (a.pos == INVALID_POS) return false;
     if (b.pos == INVALID_POS) return true;
-    const uint16_t e = tab[(a.pos % X) * X + (b.pos % X)];
+    const uint16_t e = tab[a.res * X + b.res];
     return pick<D>(a, e & 0xffu) < pick<D>(b, e >> 8);
 }
 
@@ -91,6 +95,7 @@ template <int D>
 __device__ __forceinline__ Rec<D> shfl_xor_rec(const Rec<D>& a, int j) {
     Rec<D> o;
     o.pos = __shfl_xor_sync(0xffffffffu, a.pos, j);
+    o.res = __shfl_xor_sync(0xffffffffu, a.res, j);
 #pragma unroll
     for (int k = 0; k < D; k++) o.r[k] = __shfl_xor_sync(0xffffffffu, a.r[k], j);
     return o;
@@ -103,13 +108,25 @@ __device__ __forceinline__ void load_dc_smem(const DcDev& dc, uint16_t* tab, uin
     __syncthreads();
 }
 
+// Dynamic shared memory of k_tie_pair / k_tie_warp: the X*X comparator table
+// and next_rank, sized for the level's X (a static MAX_X table would take 35 KB
+// and cut the CTAs per SM for small covers).
+__host__ __device__ inline size_t tie_tab_smem(uint32_t X) { return (((size_t)X * X * 2 + 15) & ~(size_t)15) + MAX_X * 4; }
+
+__device__ __forceinline__ void tie_tab_ptrs(uint32_t X, uint16_t*& tab, uint32_t*& nr) {
+    extern __shared__ __align__(16) uint8_t s_tab_dyn[];
+    tab = reinterpret_cast<uint16_t*>(s_tab_dyn);
+    nr = reinterpret_cast<uint32_t*>(s_tab_dyn + (((size_t)X * X * 2 + 15) & ~(size_t)15));
+}
+
 // Groups of exactly two elements, one per thread: the comparator needs one
 // cover rank of each suffix, so only those two ranks are read.
 __global__ __launch_bounds__(256) void k_tie_pair(const uint32_t* __restrict__ gstart, uint64_t ngroups,
                                                   uint32_t* __restrict__ sa, const uint32_t* __restrict__ rank_text,
                                                   const DcDev* __restrict__ dcp, TieSeg ts) {
-    __shared__ uint16_t tab[MAX_X * MAX_X];
-    __shared__ uint32_t nr[MAX_X];
+    uint16_t* tab;
+    uint32_t* nr;
+    tie_tab_ptrs(dcp->X, tab, nr);
     load_dc_smem(*dcp, tab, nr);
     const uint32_t X = dcp->X, D = dcp->D;
     const FastDiv fx = dcp->fx;
@@ -138,8 +155,9 @@ __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ g
                                                   uint32_t ngroups, uint32_t* __restrict__ sa,
                                                   const uint32_t* __restrict__ rank_text, const DcDev* __restrict__ dcp,
                                                   TieSeg ts) {
-    __shared__ uint16_t tab[MAX_X * MAX_X];
-    __shared__ uint32_t nr[MAX_X];
+    uint16_t* tab;
+    uint32_t* nr;
+    tie_tab_ptrs(dcp->X, tab, nr);
     load_dc_smem(*dcp, tab, nr);
     const uint32_t X = dcp->X;
     const uint32_t lane = threadIdx.x & 31;
@@ -154,7 +172,7 @@ __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ g
         valid = l < gsize[g];
         tie_bases(ts, start, pos0, slot0);
     }
-    Rec<D> a = load_rec<D>(valid ? (uint32_t)(sa[start + l] - pos0) : INVALID_POS, rank_text + slot0, X, nr);
+    Rec<D> a = load_rec<D>(valid ? (uint32_t)(sa[start + l] - pos0) : INVALID_POS, rank_text + slot0, dcp->fx, nr);
 #pragma unroll
     for (int k = 2; k <= W; k <<= 1) {
 #pragma unroll
@@ -163,9 +181,10 @@ __global__ __launch_bounds__(256) void k_tie_warp(const uint32_t* __restrict__ g
             const bool up = (k == W) ? true : ((l & k) == 0);
             const bool lower = (l & j) == 0;
             // lower lane keeps the smaller element when sorting up
+            // distinct suffixes are totally ordered, so a < b is !(b < a); for two
+            // padding records either answer leaves padding in both lanes
             const bool b_less = dc_less<D>(b, a, X, tab);
-            const bool a_less = dc_less<D>(a, b, X, tab);
-            const bool take_b = (lower == up) ? b_less : a_less;
+            const bool take_b = (lower == up) ? b_less : !b_less;
             if (take_b) a = b;
         }
     }
@@ -204,17 +223,34 @@ __global__ __launch_bounds__(THREADS) void k_tie_cta(const uint32_t* __restrict_
         const uint32_t start = gstart[g], size = gsize[g];
         uint64_t pos0, slot0;
         tie_bases(ts, start, pos0, slot0);
-        for (uint32_t i = threadIdx.x; i < (uint32_t)C; i += THREADS) {
-            const uint32_t p = i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS;
-            s_pos[i] = p;
-            s_res[i] = p == INVALID_POS ? NO_ELEM : (uint8_t)(p - fdiv(p, dcp->fx) * X);
-            s_idx[i] = (uint16_t)i;
+        // Every thread loads its C / THREADS elements and their D cover ranks with
+        // independent loads, so one group costs two memory latencies (positions,
+        // then ranks), not one per rank word.
+        constexpr int PER = C / THREADS;
+        static_assert(PER * THREADS == C, "C is a multiple of THREADS");
+        uint32_t p[PER], rk[PER][D];
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            p[j] = i < size ? (uint32_t)(sa[start + i] - pos0) : INVALID_POS;
         }
-        __syncthreads();
-        for (uint32_t t = threadIdx.x; t < size * D; t += THREADS) {  // ranks, D consecutive words per element
-            const uint32_t i = t / D, k = t - i * D;
-            const uint32_t p = s_pos[i];
-            s_rk[t] = __ldg(rank_text + slot0 + (uint64_t)fdiv(p, dcp->fx) * D + nr[s_res[i]] + k);
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            uint32_t q = 0, r = NO_ELEM;
+            if (p[j] != INVALID_POS) fdivmod(p[j], dcp->fx, q, r);
+            s_pos[i] = p[j];
+            s_res[i] = (uint8_t)r;
+            s_idx[i] = (uint16_t)i;
+            const uint32_t* src = rank_text + slot0 + (uint64_t)q * D + (r == NO_ELEM ? 0u : nr[r]);
+#pragma unroll
+            for (int k = 0; k < D; k++) rk[j][k] = p[j] != INVALID_POS ? __ldg(src + k) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+#pragma unroll
+            for (int k = 0; k < D; k++) s_rk[i * D + k] = rk[j][k];
         }
         __syncthreads();
 #pragma unroll
@@ -285,12 +321,12 @@ __global__ __launch_bounds__(256) void k_tie_merge(const uint64_t* __restrict__ 
         uint64_t pos0, slot0;
         tie_bases(ts, base, pos0, slot0);
         const uint32_t* rt = rank_text + slot0;
-        const Rec<D> me = load_rec<D>((uint32_t)(src[base + o] - pos0), rt, X, nr);
+        const Rec<D> me = load_rec<D>((uint32_t)(src[base + o] - pos0), rt, dcp->fx, nr);
         uint64_t a = p_start, b = p_end;  // count partner elements < me
         if (p_start < size) {
             while (a < b) {
                 uint64_t mid = (a + b) >> 1;
-                Rec<D> other = load_rec<D>((uint32_t)(src[base + mid] - pos0), rt, X, nr);
+                Rec<D> other = load_rec<D>((uint32_t)(src[base + mid] - pos0), rt, dcp->fx, nr);
                 if (dc_less<D>(other, me, X, tab)) a = mid + 1; else b = mid;
             }
         } else {

@@ -22,7 +22,7 @@ def pytest_configure(config):
 # (LCP, SA files, BWT, generalized SA) and the batched-DC tuning; the
 # allocation-free entry point last, in a file of its own.  Under -x a failure
 # in a consumer then never hides the state of the build it consumes.
-_SUITE_ORDER = ["test_abi", "test_oracle", "test_golden_fixtures", "test_gpu_parity", "test_gpu_batch",
+_SUITE_ORDER = ["test_abi", "test_oracle", "test_golden_fixtures", "test_gpu_parity", "test_gpu_copies", "test_gpu_batch",
                 "test_gpu_serve", "test_cli", "test_gpu_lcp", "test_gpu_safile", "test_gpu_bwt", "test_gpu_gsa",
                 "test_gpu_batch_autotune", "test_gpu_timeout", "test_distributed", "test_gpu_distributed",
                 "test_gpu_fullsize"]
