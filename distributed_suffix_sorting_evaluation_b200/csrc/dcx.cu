@@ -203,6 +203,9 @@ struct Options {
     uint32_t recursion_dc = 3;
     uint32_t small_threshold = SMALL_MAX;
     uint32_t prefix_chars = 0;
+    // key words of the round-0 prefix at recursion levels (2 or 3; the rest of
+    // the window is refined inside the tie groups)
+    uint32_t rec_prefix_words = 3;
     int trace = 0;
     uint32_t spin_limit = 1u << 24;
     // failure-detection test hook: this tile of every radix pass never publishes
@@ -725,7 +728,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
     const bool SEGK = K > 1;
     const SegView sv{K, d_start};
     const uint32_t words_full = (key_bits_k(B, L, K) + 31) / 32;
-    uint32_t kw0_max = depth == 0 ? 2 : 3;
+    uint32_t kw0_max = depth == 0 ? 2 : c.opt.rec_prefix_words;
     uint32_t P0 = std::min<uint32_t>(L, max_chars_in_bits_k(B, 32 * std::min(words_full, kw0_max), K));
     if (depth == 0 && c.level0_entropy > 0.05) {
         // Shortest byte-aligned prefix whose expected random collisions stay near
@@ -2504,6 +2507,10 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
         if (value < 0 || value > dcx::SMALL_MAX) return DCX_ERR_ARG;
         o.small_threshold = (uint32_t)value;
     } else if (s == "prefix_chars") o.prefix_chars = (uint32_t)value;
+    else if (s == "rec_prefix_words") {
+        if (value < 2 || value > 3) return DCX_ERR_ARG;
+        o.rec_prefix_words = (uint32_t)value;
+    }
     else if (s == "trace") o.trace = value != 0;
     else if (s == "spin_limit") o.spin_limit = (uint32_t)value;
     else if (s == "lookback_hold_tile") o.lookback_hold_tile = value < 0 ? 0xffffffffu : (uint32_t)value;

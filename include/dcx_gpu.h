@@ -92,6 +92,8 @@ int dcx_ctx_destroy(dcx_ctx* ctx);
  *   "small_threshold"      (texts up to this length are solved by the in-CTA
  *                           base case; default 2048, max 2048),
  *   "prefix_chars"         (chars in the first radix sort; 0 = auto),
+ *   "rec_prefix_words"     (key words of the first radix sort at recursion levels: 2 or 3;
+ *                           default 3),
  *   "trace"                (1 = keep level-0 names/unique flags for dcx_get_trace),
  *   "spin_limit"           (polls of a radix pass's look-back wait before it gives
  *                           up: the build then returns DCX_ERR_TIMEOUT and the
