@@ -1295,11 +1295,11 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
         const uint32_t Xr = c.opt.recursion_dc ? c.opt.recursion_dc : X;
         DBuf<uint32_t> rec(&c, m), kidx(&c, m);
         DBuf<uint8_t> rec_flag(&c, m);
-        k_rec_from_samples<<<grid_for(m, 256), 256, 0, c.stream>>>(m, srec.get(), dfl.get(), ls, rec.get(),
-                                                                  rec_flag.get());
+        k_rec_from_slots<<<(unsigned)div_up(slots, 256), 256, 0, c.stream>>>(slots, srec.get(), dfl.get(), ls,
+                                                                            rec.get(), rec_flag.get());
         DCX_CHECK_LAUNCH();
         c.launched();
-        c.alg(m * 13);
+        c.alg(slots * 8 + m * 5);
         // per-text discarding counts (num_ranks_after_discarding, pdcx.hpp:215-228)
         const uint32_t kept_total = device_scan<uint32_t>(c, OpKeepCount{rec_flag.get(), kidx.get()}, m);
         c.alg(m * 6);

@@ -416,26 +416,25 @@ __global__ void k_ranks_from_names(uint64_t slots, const uint64_t* __restrict__ 
 // Recursion string in (mod X, div X) order per text (DCRankIndex::cmp_mod_div,
 // compute_ranks.hpp:49-56): position qbase[s] + samples_before_s[c] + b holds
 // the name of the text's sample slot b*D + c.  rec_flag bit 0 = unique, bit 1 =
-// first element of its text's string.
-__device__ __forceinline__ void q_to_slot(uint64_t q, const LevelSeg& ls, uint32_t D, uint32_t& s, uint64_t& slot) {
-    s = ls.K > 1 ? bsearch_le(ls.qbase, ls.K, q) : 0u;
-    const uint64_t ql = q - ls.qbase[s];
-    const uint64_t* sb = ls.sb + (uint64_t)s * (D + 1);
-    uint32_t c = 0;
-    while (c + 1 < D && ql >= sb[c + 1]) c++;
-    slot = ls.rbase[s] + (ql - sb[c]) * D + c;
-}
-
-__global__ void k_rec_from_samples(uint64_t Mq, const uint64_t* __restrict__ srec, const DcFlags* __restrict__ f,
-                                   LevelSeg ls, uint32_t* __restrict__ rec, uint8_t* __restrict__ rec_flag) {
+// first element of its text's string.  The kernel walks the sample slots in
+// order (empty slots, past the last sample of their class, are skipped): the
+// records are read once, front to back, and the writes form D sequential
+// streams, where walking the string positions would read every record sector
+// once per class.  It is launched with one slot per thread, so the blocks in
+// flight fill the streams' sectors together.
+__global__ void k_rec_from_slots(uint64_t slots, const uint64_t* __restrict__ srec, const DcFlags* __restrict__ f,
+                                 LevelSeg ls, uint32_t* __restrict__ rec, uint8_t* __restrict__ rec_flag) {
     const uint32_t D = f->D;
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < Mq; q += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t s;
-        uint64_t slot;
-        q_to_slot(q, ls, D, s, slot);
-        const uint64_t r = srec[slot];
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < slots; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = srec[k];
+        if (r == SREC_EMPTY) continue;
+        const uint32_t s = ls.K > 1 ? bsearch_le(ls.rbase, ls.K, k) : 0u;
+        const uint64_t kl = k - ls.rbase[s];
+        const uint64_t b = kl / D;
+        const uint32_t c = (uint32_t)(kl - b * D);
+        const uint64_t q = ls.qbase[s] + ls.sb[(uint64_t)s * (D + 1) + c] + b;
         rec[q] = srec_name(r);
-        rec_flag[q] = (uint8_t)(srec_uniq(r) | ((q == ls.qbase[s]) ? 2u : 0u));
+        rec_flag[q] = (uint8_t)(srec_uniq(r) | (kl == 0 ? 2u : 0u));
     }
 }
 

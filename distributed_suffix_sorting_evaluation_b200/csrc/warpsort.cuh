@@ -111,7 +111,7 @@ __device__ __forceinline__ void warp_bitonic(T (&v)[E], uint32_t lane, Less less
 // group hold (max word, 0xffffffff) and sort last: positions are below 2^32 - 1,
 // so ordering by (word, position) puts them after every element.
 template <int E, typename CharT>
-__global__ __launch_bounds__(32 * WSORT_WARPS, 2) void k_refine_warpsort(
+__global__ __launch_bounds__(32 * WSORT_WARPS, 3) void k_refine_warpsort(
     const CharT* __restrict__ text, SegView sv, const uint32_t* __restrict__ segw, const uint32_t* __restrict__ gstart,
     const uint32_t* __restrict__ gsize, uint64_t ngroups, uint32_t* __restrict__ sa, uint8_t* __restrict__ head,
     RefineSegPlan plan) {
