@@ -33,3 +33,18 @@ def test_copies_equal_libsais(ctx, oracle, copies, sub, indel, dc):
     got = ctx.build_sa(text, dc=dc, sa_width=32)
     want = oracle.libsais(text).astype(np.uint64)
     assert np.array_equal(got.astype(np.uint64), want), (copies, sub, dc)
+
+
+def test_copies_refined_at_recursion_levels(ctx, oracle):
+    """With a 2-word first sort at the recursion levels (rec_prefix_words = 2),
+    the DC3 levels refine their tie groups by the third name: the 32-bit-char
+    forms of the warp-per-group refinement."""
+    # names past 2^21 (a 16 M-char random part) make three names wider than two
+    # key words; 50 copies of a 50 K base give level-1 groups of about 50
+    text = np.concatenate([W.iid(16 << 20, b"ACGT", seed=78), _copies(50, 50_000, 0.001, 0.0001, seed=77)])
+    ctx.set_option("rec_prefix_words", 2)
+    try:
+        got = ctx.build_sa(text, dc=39, sa_width=32)
+    finally:
+        ctx.set_option("rec_prefix_words", 3)
+    assert np.array_equal(got.astype(np.uint64), oracle.libsais(text).astype(np.uint64))
