@@ -372,7 +372,19 @@ template <typename T, typename Op>
 static T device_scan(Ctx& c, const Op& op, uint64_t n) {
     if (n == 0) return T(0);
     const uint64_t tiles = div_up(n, SCAN_TILE);
-    const uint64_t tpc = div_up(tiles, 148 * 6);  // tiles per CTA: about six CTAs per SM
+    // One chunk of tiles per CTA, as many CTAs as the rescan kernel keeps
+    // resident (its registers decide: 3-6 per SM), so both phases run as a single
+    // wave; more chunks than that would leave a second, partly empty wave.
+    static std::atomic<int> resident{0};  // per instantiation: one Op, one pair of kernels
+    int per_sm = resident.load(std::memory_order_relaxed);
+    if (per_sm == 0) {
+        int r = 0, a = 0;
+        DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_scan_reduce<T, Op>, SCAN_THREADS, 0));
+        DCX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_scan_apply<T, Op>, SCAN_THREADS, 0));
+        per_sm = std::max(1, std::min(r, a));
+        resident.store(per_sm, std::memory_order_relaxed);
+    }
+    const uint64_t tpc = div_up(tiles, 148ull * per_sm);  // tiles per CTA
     const uint64_t chunks = div_up(tiles, tpc);
     DBuf<T> sums(&c, chunks + 1);
     k_scan_reduce<T, Op><<<(unsigned)chunks, SCAN_THREADS, 0, c.stream>>>(op, n, sums.get(), tpc);
