@@ -486,6 +486,38 @@ def run_gpu(args, world, rank, local):
                     "call": "dcx_build_bwt, device pointers"}
         del d_bwt
 
+    safile_line = None
+    if args.safile:  # SA file stream: device SA -> file (the reference's raw layout) -> device, checked
+        import shutil
+        sdir = args.safile_dir or tempfile.gettempdir()
+        nbytes = n * wb
+        free = shutil.disk_usage(sdir).free
+        if free < nbytes + (4 << 30):
+            safile_line = {"skipped": f"{free >> 30} GiB free in {sdir}; the SA file takes {nbytes >> 30} GiB"}
+        else:
+            path = os.path.join(sdir, f"dcx_sa_{os.getpid()}.bin")
+            try:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ctx.write_sa_file(path, d_sa.data_ptr(), n, width)
+                t1 = time.perf_counter()
+                d_back = torch.empty_like(d_sa)
+                torch.cuda.synchronize()
+                t2 = time.perf_counter()
+                ctx.read_sa_file(path, d_back.data_ptr(), n, width)
+                torch.cuda.synchronize()
+                t3 = time.perf_counter()
+                same = bool(torch.equal(d_back, d_sa))
+                del d_back
+                safile_line = {"write_gb_per_s": round(nbytes / (t1 - t0) / 1e9, 3),
+                               "read_gb_per_s": round(nbytes / (t3 - t2) / 1e9, 3), "bytes": nbytes,
+                               "round_trip_equal": same,
+                               "call": "dcx_write_sa_file then dcx_read_sa_file of the built SA, wall clock, "
+                                       "one file in " + sdir}
+            finally:
+                if os.path.exists(path):
+                    os.remove(path)
+
     gsa_line = None
     if args.gsa:  # generalized SA of the workload text cut into 1 MiB strings (a 0 ends each)
         d_set = d_text.clone()
@@ -581,6 +613,8 @@ def run_gpu(args, world, rank, local):
             line["bwt"] = bwt_line
         if gsa_line:
             line["gsa"] = gsa_line
+        if safile_line:
+            line["safile"] = safile_line
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             sample = min(n, args.cpu_sample_mib << 20) if args.cpu_sample_mib else n
@@ -1045,6 +1079,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lcp", action="store_true", help="also time the LCP array of the built SA")
     ap.add_argument("--bwt", action="store_true", help="also time the BWT of the built SA")
+    ap.add_argument("--safile", action="store_true",
+                    help="also time writing the built SA to a file and reading it back (dcx_write/read_sa_file)")
+    ap.add_argument("--safile-dir", default="", help="directory of that file (default: the temp directory)")
     ap.add_argument("--gsa", action="store_true",
                     help="also time the generalized SA of the text cut into 1 MiB strings")
     ap.add_argument("--recursion-dc", type=int, default=0, help="difference cover of the recursion levels")

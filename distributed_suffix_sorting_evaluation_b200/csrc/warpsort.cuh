@@ -35,14 +35,14 @@ __device__ __forceinline__ KeyPos sel(bool c, const KeyPos& a, const KeyPos& b) 
     return KeyPos{c ? a.key : b.key, c ? a.pos : b.pos};
 }
 
-struct SlotRes {  // tie-break element: slot of the group's record, residue mod X
-    uint32_t slot, res;
+struct SlotRes {  // tie-break element: offset of its cover ranks (slot * D), residue mod X
+    uint32_t rk, res;
 };
 __device__ __forceinline__ SlotRes shfl_xor_el(const SlotRes& a, int m) {
-    return SlotRes{__shfl_xor_sync(0xffffffffu, a.slot, m), __shfl_xor_sync(0xffffffffu, a.res, m)};
+    return SlotRes{__shfl_xor_sync(0xffffffffu, a.rk, m), __shfl_xor_sync(0xffffffffu, a.res, m)};
 }
 __device__ __forceinline__ SlotRes sel(bool c, const SlotRes& a, const SlotRes& b) {
-    return SlotRes{c ? a.slot : b.slot, c ? a.res : b.res};
+    return SlotRes{c ? a.rk : b.rk, c ? a.res : b.res};
 }
 
 // One step (k, j) of the network with j < E: both slots in the lane.
@@ -206,9 +206,11 @@ inline size_t tie_warpsort_smem(uint32_t X) {
 }
 
 // Groups of up to 32*E elements with equal L-char windows, ordered by the
-// difference-cover comparator (as k_tie_cta).  A lane sorts (slot, residue)
-// pairs; a comparison reads the comparator entry of the two residues and the
-// two cover ranks it names from shared memory.  Slots past the group sort last.
+// difference-cover comparator (as k_tie_cta).  A lane sorts (rank offset,
+// residue) pairs; a comparison reads the comparator entry of the two residues
+// and the two cover ranks it names from shared memory.  Slots past the group
+// hold residue 0 and ranks 0xffffffff, above every rank (ranks are below 2^31),
+// so they sort last without a test of their own.
 template <int D, int E>
 __global__ __launch_bounds__(32 * WSORT_WARPS, 2) void k_tie_warpsort(
     const uint32_t* __restrict__ gstart, const uint32_t* __restrict__ gsize, uint64_t ngroups,
@@ -248,11 +250,11 @@ __global__ __launch_bounds__(32 * WSORT_WARPS, 2) void k_tie_warpsort(
                 const uint32_t i = e * 32 + lane;
                 uint32_t q = 0, r = 0;
                 if (p[e] != INVALID_POS) fdivmod(p[e], dcp->fx, q, r);
-                v[e] = SlotRes{i, r};
+                v[e] = SlotRes{i * D, r};
                 s_pos[i] = p[e];
                 const uint32_t* src = rank_text + slot0 + (uint64_t)q * D + nr[r];
 #pragma unroll
-                for (int k = 0; k < D; k++) rk[b][k] = p[e] != INVALID_POS ? __ldg(src + k) : 0u;
+                for (int k = 0; k < D; k++) rk[b][k] = p[e] != INVALID_POS ? __ldg(src + k) : 0xffffffffu;
             }
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
@@ -266,13 +268,12 @@ __global__ __launch_bounds__(32 * WSORT_WARPS, 2) void k_tie_warpsort(
         __syncwarp();
         warp_bitonic<E>(v, lane, [&](const SlotRes& x, const SlotRes& y) {
             const uint32_t t = tab[x.res * X + y.res];
-            const bool lt = s_rk[x.slot * D + (t & 0xffu)] < s_rk[y.slot * D + (t >> 8)];
-            return x.slot < size && (y.slot >= size || lt);
+            return s_rk[x.rk + (t & 0xffu)] < s_rk[y.rk + (t >> 8)];
         });
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const uint32_t i = lane * E + e;
-            if (i < size) sa[start + i] = (uint32_t)(s_pos[v[e].slot] + pos0);
+            if (i < size) sa[start + i] = (uint32_t)(s_pos[v[e].rk / D] + pos0);
         }
         __syncwarp();  // the slice is reused by the warp's next group
     }
