@@ -700,7 +700,8 @@ def run_batch(args, world, rank, local):
         sample = [W.iid(int(m), b"ACGT", seed=2_000_000 + i) for i, m in enumerate(slens)]
         bounds = [16 << 10, 256 << 10, 2 << 20, 16 << 20]
         chosen, ms_tab = ctx.autotune_batch(sample, bounds, candidates=(3, 7, 13, 21, 39), repeats=2)
-        tuned = {"classes_max_len": bounds, "dc": chosen, "ms": ms_tab.round(3).tolist()}
+        tuned = {"classes_max_len": bounds, "dc": chosen, "ms": ms_tab.round(3).tolist(),
+                 "radix_tile": ctx.batch_tile_table()}
         del sample
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     e0 = torch.cuda.Event(enable_timing=True)
@@ -1090,7 +1091,7 @@ def main():
     ap.add_argument("--batch-count", type=int, default=20000, help="texts of the batched workload")
     ap.add_argument("--batch-chunk-mib", type=int, default=2048, help="text staged on the device per batched call")
     ap.add_argument("--batch-autotune", action="store_true",
-                    help="tune the DC per size class (dcx_autotune_batch) before the batched timing")
+                    help="tune the DC and radix tile per size class (dcx_autotune_batch) before the batched timing")
     ap.add_argument("--batch-split", default="lpt", choices=["lpt", "replicas"],
                     help="how the batched workload is split over ranks under torchrun")
     ap.add_argument("--loop-budget-s", type=float, default=60.0, help="device time for the per-text loop leg")

@@ -54,7 +54,7 @@ EXPORTED = (
     "dcx_serve_release", "dcx_serve_drain", "dcx_strerror", "dcx_dc_table", "dcx_version",
     "dcx_build_sa_noalloc", "dcx_check_sa", "dcx_serve_result_device", "dcx_serve_get_stats",
     "dcx_serve_submit_ex", "dcx_build_lcp", "dcx_shard_texts", "dcx_build_bwt",
-    "dcx_build_gsa", "dcx_set_batch_dc_table", "dcx_get_batch_dc_table", "dcx_autotune_batch",
+    "dcx_build_gsa", "dcx_set_batch_dc_table", "dcx_get_batch_dc_table", "dcx_get_batch_tile_table", "dcx_autotune_batch",
     "dcx_write_sa_file", "dcx_read_sa_file", "dcx_check_sa_file", "dcx_bwt", "dcx_sort_u32", "dcx_build_sa_u32",
 )
 
@@ -142,6 +142,7 @@ def load_library(path: str | None = None):
     lib.dcx_build_gsa.argtypes = [vp, vp, u64, i32, i32, vp, u32]
     lib.dcx_set_batch_dc_table.argtypes = [vp, vp, vp, u32]
     lib.dcx_get_batch_dc_table.argtypes = [vp, vp, vp, u32, ctypes.POINTER(u32)]
+    lib.dcx_get_batch_tile_table.argtypes = [vp, vp, u32, ctypes.POINTER(u32)]
     lib.dcx_autotune_batch.argtypes = [vp, vp, vp, u32, vp, u32, vp, u32, u32, vp, vp]
     lib.dcx_write_sa_file.argtypes = [vp, ctypes.c_char_p, vp, u64, i32, u64]
     lib.dcx_read_sa_file.argtypes = [vp, ctypes.c_char_p, vp, u64, i32, u64]
@@ -319,6 +320,14 @@ class Context:
         dc = np.zeros(max(cnt.value, 1), np.int32)
         _check(self.lib.dcx_get_batch_dc_table(self.h, ml.ctypes.data, dc.ctypes.data, cnt.value, ctypes.byref(cnt)))
         return [(int(ml[i]), int(dc[i])) for i in range(cnt.value)]
+
+    def batch_tile_table(self):
+        """Radix tile (elements) of every class of the batch DC table."""
+        cnt = ctypes.c_uint32()
+        _check(self.lib.dcx_get_batch_tile_table(self.h, None, 0, ctypes.byref(cnt)))
+        t = np.zeros(max(cnt.value, 1), np.uint32)
+        _check(self.lib.dcx_get_batch_tile_table(self.h, t.ctypes.data, cnt.value, ctypes.byref(cnt)))
+        return [int(t[i]) for i in range(cnt.value)]
 
     def autotune_batch(self, texts, class_max_len, candidates=(3, 7, 13, 21, 39), repeats: int = 3):
         """Times each candidate DC on the sample texts of each size class and

@@ -206,6 +206,8 @@ struct Options {
     // key words of the round-0 prefix at recursion levels (2 or 3; the rest of
     // the window is refined inside the tie groups)
     uint32_t rec_prefix_words = 3;
+    // items per thread of a radix tile: 16 (4096-element tiles, the default) or 12 (3072)
+    uint32_t radix_items = ONESWEEP_ITEMS;
     int trace = 0;
     uint32_t spin_limit = 1u << 24;
     // failure-detection test hook: this tile of every radix pass never publishes
@@ -215,6 +217,10 @@ struct Options {
     // DC per size class of batched builds with dc_or_auto = 0: (longest text of
     // the class, X), ascending; longer texts and an empty table use DC39
     std::vector<std::pair<uint64_t, uint32_t>> batch_dc;
+    // radix tile items per class of batch_dc (empty: the context's radix_items);
+    // the autotuner fills it when batch_tune_tiles is set
+    std::vector<uint32_t> batch_items;
+    int batch_tune_tiles = 1;
     // serving
     uint32_t serve_lanes = 1;
     uint64_t serve_budget = 0;  // 0 = the context budget
@@ -465,8 +471,8 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s, int dig
         }
     }
     if (run.empty()) return 0;
-    constexpr int TILE = ONESWEEP_TILE;
-    const uint64_t tiles = div_up(count, TILE);
+    const uint32_t items = c.opt.radix_items;
+    const uint64_t tiles = div_up(count, (uint64_t)SORT_THREADS * items);
     if (tiles > c.lookback_tiles) {
         if (c.d_lookback) DCX_CUDA(cudaFree(c.d_lookback));
         c.d_lookback = nullptr;
@@ -484,13 +490,17 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s, int dig
     cudaEventCreate(&e1);
     cudaEventRecord(e0, c.stream);
     int cur = 0;
-    const size_t smem = onesweep_smem(kw);
-    static bool attr_set = false;  // the attribute is per function, the same for every context
-    if (!attr_set) {
-        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(1)));
-        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(2)));
-        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(3)));
-        attr_set = true;
+    const size_t smem = onesweep_smem(kw, items);
+    static std::atomic<bool> attr_set{false};  // the attribute is per function, the same for every context
+    if (!attr_set.load()) {
+        constexpr int I0 = ONESWEEP_ITEMS, I1 = ONESWEEP_ITEMS_ALT;
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<1, I0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(1, I0)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<2, I0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(2, I0)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<3, I0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(3, I0)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<1, I1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(1, I1)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<2, I1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(2, I1)));
+        DCX_CUDA(cudaFuncSetAttribute(k_onesweep<3, I1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(3, I1)));
+        attr_set.store(true);
     }
     // full tiles are staged with 16-byte copies: every buffer comes from the
     // context's allocator, which aligns to 256 bytes
@@ -522,9 +532,15 @@ static int radix_sort(Ctx& c, uint32_t kw, uint64_t count, SortSpace& s, int dig
         a.spin_limit = c.opt.spin_limit;
         a.hold_tile = c.opt.lookback_hold_tile;
         a.gave_up = c.d_err + 1;
-        if (kw == 1) k_onesweep<1><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
-        else if (kw == 2) k_onesweep<2><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
-        else k_onesweep<3><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+        if (items == ONESWEEP_ITEMS) {
+            if (kw == 1) k_onesweep<1, ONESWEEP_ITEMS><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+            else if (kw == 2) k_onesweep<2, ONESWEEP_ITEMS><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+            else k_onesweep<3, ONESWEEP_ITEMS><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+        } else {
+            if (kw == 1) k_onesweep<1, ONESWEEP_ITEMS_ALT><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+            else if (kw == 2) k_onesweep<2, ONESWEEP_ITEMS_ALT><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+            else k_onesweep<3, ONESWEEP_ITEMS_ALT><<<(unsigned)tiles, SORT_THREADS, smem, c.stream>>>(a);
+        }
         DCX_CHECK_LAUNCH();
         cur ^= 1;
     }
@@ -1725,6 +1741,13 @@ static uint32_t batch_x_for(const Options& o, uint64_t len) {
     return 39u;
 }
 
+// Radix tile items of a text's size class (the context's default past the table).
+static uint32_t batch_items_for(const Options& o, uint64_t len) {
+    for (size_t i = 0; i < o.batch_dc.size(); i++)
+        if (len <= o.batch_dc[i].first) return i < o.batch_items.size() ? o.batch_items[i] : o.radix_items;
+    return o.radix_items;
+}
+
 static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, uint32_t K, int dc_or_auto, int width,
                         void* sa_out, uint32_t flags) {
     if (!(width == 32 || width == 40 || width == 64)) throw Error(DCX_ERR_ARG, "sa_width must be 32, 40 or 64");
@@ -1861,16 +1884,26 @@ static void build_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets, u
         };
         run_group(small, small_ids, X);
         if (by_class) {
-            // one group per X of the size-class table, each a level of its own
-            std::map<uint32_t, std::pair<Segs, std::vector<uint32_t>>> by_x;
+            // one group per (X, radix tile) of the size-class table, each a level of its own
+            std::map<std::pair<uint32_t, uint32_t>, std::pair<Segs, std::vector<uint32_t>>> by_x;
             for (uint32_t id : big_ids) {
                 const uint64_t len = in_off[id + 1] - in_off[id];
-                auto& e = by_x[batch_x_for(c.opt, len)];
+                auto& e = by_x[{batch_x_for(c.opt, len), batch_items_for(c.opt, len)}];
                 if (e.first.start.empty()) e.first.start = {0};
                 e.first.start.push_back(e.first.start.back() + len + 1);
                 e.second.push_back(id);
             }
-            for (const auto& kv : by_x) run_group(kv.second.first, kv.second.second, kv.first);
+            const uint32_t items0 = c.opt.radix_items;
+            try {
+                for (const auto& kv : by_x) {
+                    c.opt.radix_items = kv.first.second;
+                    run_group(kv.second.first, kv.second.second, kv.first.first);
+                }
+            } catch (...) {
+                c.opt.radix_items = items0;
+                throw;
+            }
+            c.opt.radix_items = items0;
         } else {
             run_group(big, big_ids, X);
         }
@@ -1910,6 +1943,7 @@ static void autotune_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets
         if (offsets[s + 1] < offsets[s]) throw Error(DCX_ERR_ARG, "offsets must be non-decreasing");
     repeats = std::max<uint32_t>(repeats, 1);
     std::vector<std::pair<uint64_t, uint32_t>> table;
+    std::vector<uint32_t> tiles;
     for (uint32_t i = 0; i < ncls; i++) {
         const uint64_t lo = i ? class_max[i - 1] : 0, hi = class_max[i];
         std::vector<uint64_t> offs = {0};
@@ -1947,9 +1981,31 @@ static void autotune_batch(Ctx& c, const uint8_t* texts, const uint64_t* offsets
                 chosen[i] = cand[j];
             }
         }
+        // the radix tile for the chosen X: the alternative size against the default
+        uint32_t items = c.opt.radix_items;
+        if (c.opt.batch_tune_tiles) {
+            const uint32_t items0 = c.opt.radix_items;
+            const uint32_t alt = items0 == ONESWEEP_ITEMS ? ONESWEEP_ITEMS_ALT : ONESWEEP_ITEMS;
+            std::vector<double> t;
+            try {
+                c.opt.radix_items = alt;
+                for (uint32_t r = 0; r <= repeats; r++) {
+                    build_batch(c, d_text.get(), offs.data(), Kc, chosen[i], 32, d_sa.get(), DCX_DEVICE_PTRS);
+                    if (r) t.push_back(c.st.ms_total);
+                }
+            } catch (...) {
+                c.opt.radix_items = items0;
+                throw;
+            }
+            c.opt.radix_items = items0;
+            std::sort(t.begin(), t.end());
+            if (t[t.size() / 2] < best) items = alt;
+        }
         table.push_back({hi, (uint32_t)chosen[i]});
+        tiles.push_back(items);
     }
     c.opt.batch_dc = table;
+    c.opt.batch_items = tiles;
 }
 
 // Checks that sa (n entries of `width` bits) is the suffix array of text.
@@ -2522,7 +2578,11 @@ int dcx_set_option(dcx_ctx* x, const char* name, double value) {
         if (value < 0 || value > dcx::SMALL_MAX) return DCX_ERR_ARG;
         o.small_threshold = (uint32_t)value;
     } else if (s == "prefix_chars") o.prefix_chars = (uint32_t)value;
-    else if (s == "rec_prefix_words") {
+    else if (s == "batch_tune_tiles") o.batch_tune_tiles = value != 0;
+    else if (s == "radix_tile") {
+        if (value != dcx::SORT_THREADS * dcx::ONESWEEP_ITEMS && value != dcx::SORT_THREADS * dcx::ONESWEEP_ITEMS_ALT) return DCX_ERR_ARG;
+        o.radix_items = (uint32_t)value / dcx::SORT_THREADS;
+    } else if (s == "rec_prefix_words") {
         if (value < 2 || value > 3) return DCX_ERR_ARG;
         o.rec_prefix_words = (uint32_t)value;
     }
@@ -2708,6 +2768,7 @@ int dcx_set_batch_dc_table(dcx_ctx* x, const uint64_t* max_len, const int* dc, u
             t.push_back({max_len[i], (uint32_t)dc[i]});
         }
         x->c.opt.batch_dc = t;
+        x->c.opt.batch_items.clear();  // every class on the context's radix tile
     });
 }
 
@@ -2720,6 +2781,17 @@ int dcx_get_batch_dc_table(dcx_ctx* x, uint64_t* max_len, int* dc, uint32_t capa
         if (max_len) max_len[i] = t[i].first;
         if (dc) dc[i] = (int)t[i].second;
     }
+    return DCX_OK;
+}
+
+int dcx_get_batch_tile_table(dcx_ctx* x, uint32_t* tile_elems, uint32_t capacity, uint32_t* count) {
+    if (!x || !count) return DCX_ERR_ARG;
+    std::lock_guard<std::mutex> lk(x->c.build_mu);
+    const auto& o = x->c.opt;
+    *count = (uint32_t)o.batch_dc.size();
+    for (uint32_t i = 0; i < capacity && i < o.batch_dc.size(); i++)
+        if (tile_elems)
+            tile_elems[i] = dcx::SORT_THREADS * (i < o.batch_items.size() ? o.batch_items[i] : o.radix_items);
     return DCX_OK;
 }
 

@@ -3,7 +3,9 @@
 // distributed comparison sorts (lightweight_dcx/src/sorters/sorting_wrapper.hpp:57-94,
 // sample_sort.hpp:36-171) for every sort of the DCX pipeline.
 //
-// One kernel per 8-bit digit (k_onesweep<KW>, 4096-element tiles, three CTAs per SM):
+// One kernel per 8-bit digit (k_onesweep<KW, ITEMS>: 4096-element tiles with three CTAs
+// per SM by default, 3072-element tiles with four as the alternative a context
+// option or the batch autotuner selects):
 //   * tiles are claimed in order through an atomic counter;
 //   * the words the pass does not rank on (other key words, the value) are
 //     prefetched into shared memory with cp.async as soon as the tile is
@@ -88,14 +90,18 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-constexpr int ONESWEEP_ITEMS = 16;  // 4096-element tiles
+constexpr int ONESWEEP_ITEMS = 16;      // default: 4096-element tiles
+constexpr int ONESWEEP_ITEMS_ALT = 12;  // alternative: 3072-element tiles
 constexpr int ONESWEEP_TILE = SORT_THREADS * ONESWEEP_ITEMS;
-constexpr int ONESWEEP_MIN_CTAS = 3;  // register budget: three 256-thread CTAs per SM
 
-// Dynamic shared memory of k_onesweep<KW>: the exchange buffer plus one staging
-// buffer per carried array (KW - 1 other key words and the value).
-__host__ __device__ constexpr size_t onesweep_smem(uint32_t kw) {
-    return sizeof(uint32_t) * (size_t)ONESWEEP_TILE * (1 + kw);
+// Register budget of a tile size: three 256-thread CTAs per SM for 16 items per
+// thread, four for 12.
+__host__ __device__ constexpr int onesweep_min_ctas(int items) { return items > 12 ? 3 : 4; }
+
+// Dynamic shared memory of k_onesweep<KW, ITEMS>: the exchange buffer plus one
+// staging buffer per carried array (KW - 1 other key words and the value).
+__host__ __device__ constexpr size_t onesweep_smem(uint32_t kw, uint32_t items = ONESWEEP_ITEMS) {
+    return sizeof(uint32_t) * (size_t)SORT_THREADS * items * (1 + kw);
 }
 
 // Shared state of one CTA of k_onesweep (static shared memory).
@@ -271,9 +277,9 @@ __device__ __forceinline__ void onesweep_tile(const SortPassArgs& a, OnesweepSha
 // One LSD pass over KW key words (1..3) carrying one value.  Every array base
 // must be 16-byte aligned (full tiles are staged with 16-byte copies; the last,
 // partial tile uses 4-byte copies, which never read past the array end).
-template <int KW>
-__global__ __launch_bounds__(SORT_THREADS, ONESWEEP_MIN_CTAS) void k_onesweep(SortPassArgs a) {
-    constexpr int TILE = ONESWEEP_TILE;
+template <int KW, int ITEMS>
+__global__ __launch_bounds__(SORT_THREADS, onesweep_min_ctas(ITEMS)) void k_onesweep(SortPassArgs a) {
+    constexpr int TILE = SORT_THREADS * ITEMS;
     __shared__ OnesweepShared sm;
     extern __shared__ __align__(16) uint32_t s_dyn[];
     const int tid = threadIdx.x;
@@ -287,9 +293,9 @@ __global__ __launch_bounds__(SORT_THREADS, ONESWEEP_MIN_CTAS) void k_onesweep(So
     const uint64_t remain = a.n - tile * TILE;
     const uint32_t tile_valid = remain < (uint64_t)TILE ? (uint32_t)remain : (uint32_t)TILE;
     if (tile_valid == (uint32_t)TILE)
-        onesweep_tile<KW, ONESWEEP_ITEMS, true>(a, sm, s_dyn, s_dyn + TILE, tile, tile_valid);
+        onesweep_tile<KW, ITEMS, true>(a, sm, s_dyn, s_dyn + TILE, tile, tile_valid);
     else
-        onesweep_tile<KW, ONESWEEP_ITEMS, false>(a, sm, s_dyn, s_dyn + TILE, tile, tile_valid);
+        onesweep_tile<KW, ITEMS, false>(a, sm, s_dyn, s_dyn + TILE, tile, tile_valid);
 }
 
 // Histogram of every 8-bit digit of keys already in memory (4*kw passes), for

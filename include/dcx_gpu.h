@@ -94,6 +94,10 @@ int dcx_ctx_destroy(dcx_ctx* ctx);
  *   "prefix_chars"         (chars in the first radix sort; 0 = auto),
  *   "rec_prefix_words"     (key words of the first radix sort at recursion levels: 2 or 3;
  *                           default 3),
+ *   "radix_tile"           (elements per tile of every radix pass: 4096, the default,
+ *                           or 3072),
+ *   "batch_tune_tiles"     (1 = dcx_autotune_batch also chooses the radix tile per class;
+ *                           default 1),
  *   "trace"                (1 = keep level-0 names/unique flags for dcx_get_trace),
  *   "spin_limit"           (polls of a radix pass's look-back wait before it gives
  *                           up: the build then returns DCX_ERR_TIMEOUT and the
@@ -241,6 +245,10 @@ int dcx_build_sa_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offse
 int dcx_set_batch_dc_table(dcx_ctx* ctx, const uint64_t* max_len, const int* dc, uint32_t count);
 /* Copies up to `capacity` entries of the table; *count = its length. */
 int dcx_get_batch_dc_table(dcx_ctx* ctx, uint64_t* max_len, int* dc, uint32_t capacity, uint32_t* count);
+/* Radix tile (elements per tile: 4096 or 3072) of every class of that table,
+ * as the autotuner chose it; dcx_set_batch_dc_table resets every class to the
+ * context's tile (option "radix_tile").  *count = the table's length. */
+int dcx_get_batch_tile_table(dcx_ctx* ctx, uint32_t* tile_elems, uint32_t capacity, uint32_t* count);
 /* Autotuner of that table.  The texts of a sample batch in HOST memory (layout
  * of dcx_build_sa_batch) are split into size classes (length in
  * (class_max_len[i-1], class_max_len[i]]); each class is built as one batch
@@ -248,8 +256,11 @@ int dcx_get_batch_dc_table(dcx_ctx* ctx, uint64_t* max_len, int* dc, uint32_t ca
  * runs (device time, median), and the fastest X of each class is installed as
  * the table.  chosen_dc[num_classes] receives the choices (0 for a class
  * without sample texts, which keeps DC39); ms_out[num_classes *
- * num_candidates] (may be null) the medians in ms (-1 for such a class).  No
- * counterpart in the reference, whose cli takes --dcx per run. */
+ * num_candidates] (may be null) the medians in ms (-1 for such a class).  With
+ * the option "batch_tune_tiles" (default 1) the chosen X of each class is also
+ * timed with the other radix tile (3072 against 4096 elements), and the faster
+ * tile is installed beside it (dcx_get_batch_tile_table).  No counterpart in
+ * the reference, whose cli takes --dcx per run. */
 int dcx_autotune_batch(dcx_ctx* ctx, const uint8_t* texts, const uint64_t* offsets, uint32_t num_texts,
                        const uint64_t* class_max_len, uint32_t num_classes, const int* candidates,
                        uint32_t num_candidates, uint32_t repeats, int* chosen_dc, double* ms_out);
