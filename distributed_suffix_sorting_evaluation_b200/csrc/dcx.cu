@@ -595,12 +595,36 @@ struct TieGroups {
 
 static TieGroups bin_groups(Ctx& c, uint64_t G, const uint32_t* starts, const uint32_t* ends);
 
-static TieGroups group_ties(Ctx& c, const uint8_t* head, uint64_t N) {
+static TieGroups group_ties_scan(Ctx& c, const uint8_t* head, uint64_t N) {
     DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1);
     OpGroups op{head, N, starts.get(), ends.get()};
     const uint64_t tot = device_scan<uint64_t>(c, op, N);
     c.alg(N);
     return bin_groups(c, tot & 0xffffffffull, starts.get(), ends.get());
+}
+
+// Tie groups of all N head flags.  When few elements are tied (`tied`, the
+// count of flags 0, below N/8) the groups are found by walking from each group
+// start (k_groups_walk, one read of the flags), falling back to the scan when a
+// group is longer than the walk's limit.  When most are tied, the scan: a walk
+// per group then costs more than the scan, and the scan lists the groups in
+// array order, which the group sorts that follow read with better locality.
+static TieGroups group_ties(Ctx& c, const uint8_t* head, uint64_t N, uint64_t tied) {
+    if (((uintptr_t)head & 15) != 0 || tied >= N / 8) return group_ties_scan(c, head, N);
+    constexpr uint32_t WALK_LIMIT = 1u << 16;
+    DBuf<uint32_t> starts(&c, N / 2 + 1), ends(&c, N / 2 + 1), cnt(&c, 2);
+    DCX_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, c.stream));
+    k_groups_walk<<<grid_for(div_up(N, 16), 256, 148 * 8), 256, 0, c.stream>>>(N, head, WALK_LIMIT, starts.get(),
+                                                                                ends.get(), cnt.get(), cnt.get() + 1);
+    DCX_CHECK_LAUNCH();
+    c.launched();
+    c.alg(N + N / 8);
+    uint32_t h[2];
+    DCX_CUDA(cudaMemcpyAsync(h, cnt.get(), 8, cudaMemcpyDeviceToHost, c.stream));
+    DCX_CUDA(cudaStreamSynchronize(c.stream));
+    if (h[1]) return group_ties_scan(c, head, N);
+    if (h[0] > N / 2 + 1) throw Error(DCX_ERR_INTERNAL, "more tie groups than the bound");
+    return bin_groups(c, h[0], starts.get(), ends.get());
 }
 
 // Tie groups found inside parent groups that hold every tie (the round-0
@@ -870,7 +894,7 @@ static void sort_windows(Ctx& c, const CharT* text, const Segs& sg, const uint64
         const uint32_t cpw = std::min<uint32_t>(sizeof(CharT) == 1 ? 64 : 16, max_chars_in_bits(B, 64));
         const uint32_t W = (rem + cpw - 1) / cpw;
         if (W <= (uint32_t)RSEG_MAX_W) {
-            tg = group_ties(c, hd, N);
+            tg = group_ties(c, hd, N, round0_ties);
             RefineSegPlan plan{};
             plan.W = W;
             for (uint32_t w = 0; w < W; w++) {
@@ -1103,7 +1127,7 @@ static void tie_break_d(Ctx& c, uint32_t* sa, uint64_t N, const uint32_t* rank_t
 
 static void tie_break(Ctx& c, uint32_t* sa, const uint8_t* head, uint64_t N, const uint32_t* rank_text,
                       const DcHost& dc, TieSeg ts, const TieGroups* parents) {
-    TieGroups tg = parents ? group_ties_within(c, head, *parents) : group_ties(c, head, N);
+    TieGroups tg = parents ? group_ties_within(c, head, *parents) : group_ties_scan(c, head, N);
     const uint64_t G = tg.G;
     if (G == 0) return;
     const std::vector<uint32_t>& counts = tg.counts;

@@ -719,6 +719,76 @@ __global__ void k_subgroups(uint64_t Gp, const uint32_t* __restrict__ pstart, co
     }
 }
 
+// Tie groups of a whole head-flag array (flags 16-byte aligned) without a scan:
+// thread t reads flags [16t, 16t + 16) with one 16-byte load plus the flag after
+// them, finds the group starts among them (a flag 1 followed by a 0; position N
+// counts as a 1), and walks each group to its end: inside its own 16 flags from
+// registers, past them byte by byte, at most `limit` flags.  A longer group
+// sets *overflow (its entry is then incomplete and the caller scans instead).
+// Groups are appended as (start, end) in any order, one atomic reservation per
+// warp; every lane runs the same number of rounds.
+__global__ void k_groups_walk(uint64_t N, const uint8_t* __restrict__ head, uint32_t limit,
+                              uint32_t* __restrict__ out_start, uint32_t* __restrict__ out_end,
+                              uint32_t* __restrict__ count, uint32_t* __restrict__ overflow) {
+    const uint64_t blocks = (N + 15) / 16;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t first = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t rounds = (blocks + stride - 1) / stride;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t r = 0; r < rounds; r++) {
+        const uint64_t t = first + r * stride;
+        const uint64_t i0 = t * 16;
+        uint32_t f = 0;  // bit k: flag of i0 + k (k = 0..16); positions >= N count as 1
+        if (t < blocks) {
+            if (i0 + 16 <= N) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(head + i0));
+                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        if ((w[q] >> (8 * b)) & 0xffu) f |= 1u << (4 * q + b);
+            } else {
+                for (uint32_t k = 0; k < 16; k++) f |= (i0 + k >= N || head[i0 + k]) ? 1u << k : 0u;
+            }
+            f |= (i0 + 16 >= N || head[i0 + 16]) ? 1u << 16 : 0u;
+        }
+        // starts: flag 1 at k, flag 0 at k + 1 (k = 0..15)
+        const uint32_t st = t < blocks ? (f & ~(f >> 1)) & 0xffffu : 0u;
+        const uint32_t nsub = __popc(st);
+        uint32_t incl = nsub;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += x;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t base = 0;
+        if (lane == 31 && total) base = atomicAdd(count, total);
+        base = __shfl_sync(0xffffffffu, base, 31) + incl - nsub;
+        uint32_t s = st;
+        while (s) {
+            const uint32_t k = __ffs(s) - 1;
+            s &= s - 1;
+            // the group runs from i0 + k to the position before the next flag 1
+            const uint32_t later = (f >> (k + 1)) & 0x1ffffu;  // flags of i0 + k + 1 .. i0 + 16
+            uint64_t end;
+            if (later) {
+                end = i0 + k + __ffs(later) - 1;  // next 1 within the 17 flags
+            } else {
+                uint64_t p = i0 + 17;
+                const uint64_t stop = i0 + k + 1 + (uint64_t)limit;
+                while (p < N && p < stop && !head[p]) p++;
+                if (p < N && p >= stop) atomicOr(overflow, 1u);
+                end = p - 1;
+            }
+            out_start[base] = (uint32_t)(i0 + k);
+            out_end[base] = (uint32_t)end;
+            base++;
+        }
+    }
+}
+
 // Bins tie groups by size class.  Cursor updates are aggregated per warp: the
 // lanes holding the same class elect one lane that reserves their slots.
 __global__ void k_tie_bin(uint64_t G, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,

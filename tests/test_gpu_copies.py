@@ -48,3 +48,17 @@ def test_copies_refined_at_recursion_levels(ctx, oracle):
     finally:
         ctx.set_option("rec_prefix_words", 3)
     assert np.array_equal(got.astype(np.uint64), oracle.libsais(text).astype(np.uint64))
+
+
+@pytest.mark.parametrize("dc", [3, 39])
+def test_tie_groups_longer_than_the_walk(ctx, oracle, dc):
+    """Round-0 tie groups of more than 65,536 elements: texts that are almost
+    all tied (a run of one character, a short period) take the scan; a random
+    text with one long run has few ties, so its groups are walked from their
+    starts until the run's group outgrows the walk and the scan takes over."""
+    rng = np.random.default_rng(21)
+    with_run = np.concatenate([rng.integers(65, 69, 500_000), np.full(100_000, 65), rng.integers(65, 69, 500_000)])
+    for text in (np.full(300_000, ord("A"), np.uint8), np.tile(np.frombuffer(b"ACGT", np.uint8), 100_000),
+                 with_run.astype(np.uint8)):
+        got = ctx.build_sa(text, dc=dc, sa_width=32)
+        assert np.array_equal(got.astype(np.uint64), oracle.libsais(text).astype(np.uint64)), (text.size, dc)
