@@ -40,3 +40,27 @@ def test_zipf256_uses_every_byte_value():
     counts = np.bincount(z, minlength=256)
     assert (counts > 0).all()  # sigma = 256: the reference cli refuses this text
     assert 0.15 < counts.max() / z.size < 0.3  # the most frequent symbol under s = 1.1
+
+
+def test_profiling_size_keeps_the_copy_count():
+    """bench.py --text-mib 256 --base-kib 1280 shrinks the 2 GiB pangenome to 256
+    MiB with the full-size copy count (the tie groups of ~204 elements that the
+    profiling captures of the group sorts need)."""
+    import argparse
+    import importlib.util
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    args = argparse.Namespace(workload="cfg3a_dc39_pangenome_2GiB", text_mib=256, base_kib=1280)
+    w, gen_kw, label = bench._single_workload(args)
+    assert w["n"] == 256 << 20 and gen_kw == {"base_len": 1280 << 10}
+    assert label == "cfg3a_dc39_pangenome_2GiB@256MiB,base1280KiB"
+    t = getattr(W, w["gen"])(w["n"], seed=w["seed"], **gen_kw)
+    full_copies = (2 << 30) // ((10 << 20) + 1)
+    assert abs(int(np.count_nonzero(t == ord("$"))) - full_copies) <= 2
+    # the base option applies to the pangenome generator only
+    w2, gen_kw2, _ = bench._single_workload(argparse.Namespace(workload="cfg2_dc39_markov_dna_1GiB",
+                                                               text_mib=0, base_kib=1280))
+    assert gen_kw2 == {} and w2["n"] == 1 << 30
