@@ -1453,26 +1453,31 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
             }
             sa2.reset();
             if (any_discard) {
-                // non-unique samples of discarding texts: sort by (name, rank2) (pdcx.hpp:296-346)
-                const uint32_t mu = device_scan<uint32_t>(
-                    c, OpNonUniqueSeg{srec.get(), dfl.get(), ls, kidx.get(), rank_of.get(), nullptr, nullptr, nullptr},
-                    slots);
+                // non-unique samples of discarding texts: sort by (name, rank2) (pdcx.hpp:296-346).
+                // One scan compacts them into first buffers sized for every sample
+                // (their count is not known before it); the second buffers get the count.
+                DBuf<uint32_t> keys[2][2];
+                DBuf<uint32_t> vals[2];
+                SortSpace s;
+                for (int w = 0; w < 2; w++) {
+                    keys[0][w] = DBuf<uint32_t>(&c, m);
+                    s.k[0][w] = keys[0][w].get();
+                }
+                vals[0] = DBuf<uint32_t>(&c, m);
+                s.v[0] = vals[0].get();
+                const uint32_t mu = device_scan<uint32_t>(c, OpNonUniqueSeg{srec.get(), dfl.get(), ls, kidx.get(),
+                                                                          rank_of.get(), s.k[0][0], s.k[0][1],
+                                                                          s.v[0]},
+                                                          slots);
+                if (mu > m) throw Error(DCX_ERR_INTERNAL, "more non-unique samples than samples");
                 if (mu) {
-                    DBuf<uint32_t> keys[2][2];
-                    DBuf<uint32_t> vals[2];
-                    SortSpace s;
-                    for (int bb = 0; bb < 2; bb++) {
-                        for (int w = 0; w < 2; w++) {
-                            keys[bb][w] = DBuf<uint32_t>(&c, mu);
-                            s.k[bb][w] = keys[bb][w].get();
-                        }
-                        vals[bb] = DBuf<uint32_t>(&c, mu);
-                        s.v[bb] = vals[bb].get();
+                    for (int w = 0; w < 2; w++) {
+                        keys[1][w] = DBuf<uint32_t>(&c, mu);
+                        s.k[1][w] = keys[1][w].get();
                     }
-                    device_scan<uint32_t>(c, OpNonUniqueSeg{srec.get(), dfl.get(), ls, kidx.get(), rank_of.get(),
-                                                            s.k[0][0], s.k[0][1], s.v[0]},
-                                          slots);
-                    c.alg(slots * 9 + mu * 24);
+                    vals[1] = DBuf<uint32_t>(&c, mu);
+                    s.v[1] = vals[1].get();
+                    c.alg(slots * 9 + mu * 12);
                     rank_of.reset();
                     kidx.reset();
                     DCX_CUDA(cudaMemsetAsync(c.d_hist, 0, 16 * RADIX * 4, c.stream));
