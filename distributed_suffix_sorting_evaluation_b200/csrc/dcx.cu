@@ -1405,8 +1405,18 @@ static void level(Ctx& c, const CharT* text, const Segs& sg, uint64_t sigma, uin
             // recursion input: the kept names of every recursing text, each followed by a 0
             DBuf<uint32_t> rec2(&c, pos2);
             DCX_CUDA(cudaMemsetAsync(rec2.get(), 0, pos2 * 4, c.stream));
-            device_scan<uint32_t>(c, OpCompact{rec_flag.get(), rec.get(), ls, rec2.get(), kidx.get()}, m);
-            c.alg(m * 10 + total2 * 4);
+            if (K == 1) {
+                // one text: the kept indices are q itself (direct) or the keep-count
+                // prefix already in kidx (discarding), so an elementwise copy compacts
+                k_compact_one<<<grid_for(m, 256), 256, 0, c.stream>>>(m, rec_flag.get(), rec.get(), mode[0],
+                                                                       start2[0], rec2.get(), kidx.get());
+                DCX_CHECK_LAUNCH();
+                c.launched();
+                c.alg(m * 9 + total2 * 4);
+            } else {
+                device_scan<uint32_t>(c, OpCompact{rec_flag.get(), rec.get(), ls, rec2.get(), kidx.get()}, m);
+                c.alg(m * 10 + total2 * 4);
+            }
             rec.reset();
             rec_flag.reset();
             Segs sg2;

@@ -479,6 +479,23 @@ struct OpCompact {
     }
 };
 
+// OpCompact for a single text (K = 1) without a scan: a direct text keeps every
+// position q (kept index q), a discarding text the positions the discarding
+// rule keeps, whose kept indices the keep-count scan (OpKeepCount) already
+// wrote to kidx.
+__global__ void k_compact_one(uint64_t m, const uint8_t* __restrict__ rec_flag, const uint32_t* __restrict__ rec,
+                              uint8_t mode, uint64_t start2, uint32_t* __restrict__ rec2,
+                              uint32_t* __restrict__ kidx) {
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (uint64_t)gridDim.x * blockDim.x) {
+        if (mode == REC_DIRECT) {
+            rec2[start2 + q] = rec[q];
+            kidx[q] = (uint32_t)q;
+        } else if (mode == REC_DISCARD && discard_keep(rec_flag, q)) {
+            rec2[start2 + kidx[q]] = rec[q];
+        }
+    }
+}
+
 // Results of the recursive call.  sa2 holds, for each recursing text r (in
 // order), the suffix array of its reduced string at o2[r].  Direct texts: the
 // sample at string position q gets rank k + 1 (pdcx.hpp:183-212, map_back 83-94).
